@@ -1,0 +1,362 @@
+#!/usr/bin/env python
+"""Benchmark: exact embeddings/s of the subgraph-isomorphism hot path on B200.
+
+Workload (one step): the symmetrised R-MAT scale-22 graph (4,194,304 vertices,
+edge factor 16, a=0.57 b=0.19 c=0.19, self-loops and duplicates removed,
+32 Zipf(s=1.0) labels) resident in HBM; five labelled queries (triangle,
+4-cycle, 4-clique, 5-path, tailed triangle, labels from random walks on the
+data graph) counted exactly, one query per launch sequence, reference
+heuristic order.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
+
+Under torchrun (N > 1) every rank holds a replica of the graph and counts a
+contiguous shard of each query's level-0 candidates; counts are summed with
+one all-reduce after the timed region and the step time is the maximum over
+ranks.  `--impl reference` times the CPU port of the reference algorithm
+(the oracle, all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SHAPE_SEEDS = 2  # query i uses seed 2 + i
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["mine", "reference"], default="mine")
+    p.add_argument("--scale", type=int, default=22)
+    p.add_argument("--cpu-seconds", type=float, default=12.0,
+                   help="target CPU time of the oracle baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--e2e-steps", type=int, default=2)
+    return p.parse_args()
+
+
+def workload(scale):
+    import matrixgraph_b200 as mg
+    g = mg.rmat(scale, 16, 0.57, 0.19, 0.19, seed=0, n_labels=32, label_kind="zipf",
+                zipf_s=1.0, label_seed=1)
+    qs = [mg.query_walk(g, s, seed=SHAPE_SEEDS + i) for i, s in enumerate(mg.SHAPES)]
+    return g, qs
+
+
+def config(scale, g, extra=None):
+    import matrixgraph_b200 as mg
+    c = {"workload": f"R-MAT scale {scale} ({g.n:,} vertices, edge factor 16, a=0.57 b=0.19 "
+                     f"c=0.19, symmetrised, no self-loops/duplicates, {g.m_out:,} directed "
+                     "entries), 32 Zipf(s=1.0) labels; 5 random-walk-labelled queries "
+                     f"({', '.join(mg.SHAPES)}); one query per launch sequence, reference "
+                     "heuristic order, count mode",
+         "queries": list(mg.SHAPES), "order": "reference", "mode": "count",
+         "l2": "inputs larger than L2 (graph + indices > 1 GB) and a 256 MiB L2 flush "
+               "before every step"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}",
+                                       f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as f:
+            for line in f:
+                t = [x.strip() for x in line.split(",")]
+                if len(t) >= 9 and t[1].replace(".", "").isdigit():
+                    rows.append(t)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]),
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def first_bucket_sizes(g, qs, dg=None):
+    """Level-0 candidate count of each query (its first vertex's label bucket)."""
+    import numpy as np
+
+    import matrixgraph_b200 as mg
+    lab = g.array("labels")
+    vals, cnts = np.unique(lab, return_counts=True)
+    size = dict(zip(vals.tolist(), cnts.tolist()))
+    out = []
+    for q in qs:
+        order = mg.plan_order(q)
+        out.append(int(size.get(int(q.array("labels")[order[0]]), 0)))
+    return out
+
+
+def cpu_baseline(g, qs, target_s):
+    """The oracle (exact CPU port, all host threads) on a bounded sample of roots."""
+    import oracle as O
+    threads = os.cpu_count() or 1
+    og = O.Graph.from_csr(g)
+    total_c, total_t, parts = 0, 0.0, []
+    per_q = target_s / len(qs)
+    for q in qs:
+        oq = O.query_from_csr(q)
+        order = O.reference_order(oq)
+        nb = O.bucket_size(og, oq, order)
+        r = max(1, nb // 4096)
+        while True:
+            t0 = time.perf_counter()
+            res = O.count(og, oq, order=order, threads=threads, root_range=(0, r))
+            dt = time.perf_counter() - t0
+            if dt >= per_q / 4 or r >= nb:
+                break
+            r = min(nb, r * 4)
+        total_c += res["count"]
+        total_t += dt
+        parts.append(f"{r}/{nb}")
+    return {"value": total_c / total_t if total_t > 0 else 0.0, "unit": "embeddings/s",
+            "cores": threads, "kind": "port",
+            "sample": "oracle over the first r of each query's level-0 candidates (r/total: "
+                      + ", ".join(parts) + "), embeddings counted / wall seconds"}, og
+
+
+def run_reference(args):
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    g, qs = workload(args.scale)
+    import oracle as O
+    threads = os.cpu_count() or 1
+    og = O.Graph.from_csr(g)
+    oqs = [O.query_from_csr(q) for q in qs]
+    # Fix the per-query sample in warm-up so every timed step does the same work.
+    samples = []
+    per_q = args.cpu_seconds / len(qs)
+    for oq in oqs:
+        order = O.reference_order(oq)
+        nb = O.bucket_size(og, oq, order)
+        r = max(1, nb // 4096)
+        while True:
+            t0 = time.perf_counter()
+            O.count(og, oq, order=order, threads=threads, root_range=(0, r))
+            if time.perf_counter() - t0 >= per_q / 4 or r >= nb:
+                break
+            r = min(nb, r * 4)
+        samples.append((order, r, nb))
+    for _ in range(max(0, args.warmup - 1)):
+        pass
+    times, counts = [], 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        c = 0
+        for oq, (order, r, nb) in zip(oqs, samples):
+            c += O.count(og, oq, order=order, threads=threads, root_range=(0, r))["count"]
+        times.append(time.perf_counter() - t0)
+        counts = c
+    ms = 1e3 * statistics.mean(times)
+    value = counts / (ms / 1e3)
+    sample = ("oracle (exact CPU port of the reference algorithm) over the first r of each "
+              "query's level-0 candidates: " + ", ".join(f"{r}/{nb}" for _, r, nb in samples))
+    line = {"impl": "reference", "metric": "exact embeddings/s", "value": value,
+            "unit": "embeddings/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": config(args.scale, g, {"sample": sample}),
+            "cpu_baseline": {"value": value, "unit": "embeddings/s", "cores": threads,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "embeddings/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_mine(args):
+    import torch
+
+    import matrixgraph_b200 as mg
+    world, rank, local = dist_setup(args)
+    device = local
+    torch.cuda.set_device(device)
+    t0 = time.perf_counter()
+    g, qs = workload(args.scale)
+    gen_s = time.perf_counter() - t0
+    buckets = first_bucket_sizes(g, qs)
+    ranges = [mg.shard_roots(nb, rank, world) if world > 1 else None for nb in buckets]
+    dg = mg.DeviceGraph(g, device)
+    info = dg.info
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device=f"cuda:{device}")
+
+    def step(collect):
+        flush.zero_()
+        torch.cuda.synchronize(device)
+        ms, launches, balg, balgc, counts = 0.0, 0, 0, 0, []
+        for q, rr in zip(qs, ranges):
+            c, st = dg.count(q, stats=True, root_range=rr)
+            ms += st["device_ms"]
+            launches += st["launches"]
+            balg += st["balg_bytes"]
+            balgc += st["balg_count_bytes"]
+            counts.append(c)
+        if collect is not None:
+            collect.append((ms, launches, balg, balgc, counts))
+
+    for _ in range(args.warmup):
+        step(None)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(device)
+    clk = Clocks(device)
+    clk.start()
+    recs = []
+    host0 = time.perf_counter()
+    for _ in range(args.steps):
+        step(recs)
+    torch.cuda.synchronize(device)
+    host_ms = 1e3 * (time.perf_counter() - host0) / args.steps
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = clk.stop()
+    ms_step = statistics.mean(r[0] for r in recs)
+    counts = recs[-1][4]
+    launches = recs[-1][1]
+    balgc = recs[-1][3]
+    balg = recs[-1][2]
+    if world > 1:
+        t = torch.tensor([ms_step], dtype=torch.float64, device=f"cuda:{device}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_step = float(t.item())
+        c = torch.tensor(counts + [balgc, balg, launches], dtype=torch.int64,
+                         device=f"cuda:{device}")
+        torch.distributed.all_reduce(c)
+        vals = c.tolist()
+        counts, balgc, balg, launches = vals[:len(qs)], vals[-3], vals[-2], vals[-1]
+    emb = sum(counts)
+    value = emb / (ms_step / 1e3)
+
+    # End to end through the public API from host buffers: upload (graph
+    # arrays host -> device, derived indices), five counts, counts back.
+    e2e_times = []
+    h2d = (g.n + 1) * 4 + g.m_out * 4 + 4 * g.n * 3 + sum(q.n * 4 * 4 + q.m_out * 8 for q in qs)
+    d2h = 8 * len(qs)
+    for _ in range(args.e2e_steps):
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        dg2 = mg.DeviceGraph(g, device)
+        for q, rr in zip(qs, ranges):
+            dg2.count(q, root_range=rr)
+        dg2.free()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = statistics.median(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{device}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    peak, peak_kind = peaks()
+    achieved = balgc / (ms_step / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None,
+                "basis": f"B_alg (count-mode definition) per step / device time per step; "
+                         f"peak {peak_kind} copy bandwidth",
+                "balg_count_bytes_per_step": balgc, "balg_bytes_per_step": balg}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu, _ = cpu_baseline(g, qs, args.cpu_seconds)
+    if rank == 0:
+        line = {"metric": "exact embeddings/s", "value": value, "unit": "embeddings/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+                "config": config(args.scale, g), "queries_per_s": len(qs) / (ms_step / 1e3),
+                "counts": counts, "host_ms_per_step": host_ms,
+                "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": {"value": emb / e2e_s, "unit": "embeddings/s",
+                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "seconds_per_step": e2e_s},
+                "clocks": clocks, "gpu_launches": launches * args.steps,
+                "graph": {"n": info["n"], "m_out": info["m_out"],
+                          "device_bytes": info["device_bytes"], "max_degree": info["max_degree"],
+                          "gen_seconds": gen_s}}
+        print(json.dumps(line), flush=True)
+    dg.free()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_mine(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,246 @@
+/*
+ * mg_subiso.h — C-ABI of the B200 subgraph-isomorphism engine (libmg_subiso.so).
+ *
+ * Plain C: host pointers, sizes and integer status codes only; no CUDA or
+ * torch types cross this boundary.  Every entry point returns MG_OK (0) or a
+ * negative MG_E_* code and never calls exit()/abort(); the message of the
+ * last failure on the calling thread is returned by mg_last_error().
+ *
+ * Each entry point names the reference interface it replaces
+ * (hsiaoko/MatrixGraph, paths relative to the project root).
+ *
+ * Semantics of a "match" (all entry points): an injective map f from query
+ * vertices to data vertices with label(f(u)) == label(u) for every query
+ * vertex u and (f(u), f(w)) an edge of the data graph for every directed
+ * query edge (u, w).  Non-induced; automorphic images are counted
+ * separately.  Edge multiplicity is ignored (set semantics).  This is the
+ * matching rule of the reference's only exact GPU matcher,
+ * core/task/gpu_task/kernel/kernel_gar_match.cu:305-363.
+ */
+#ifndef MG_SUBISO_H_
+#define MG_SUBISO_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define MG_OK          0
+#define MG_E_IO       -1   /* file missing / unreadable / unwritable          */
+#define MG_E_FORMAT   -2   /* malformed meta.yaml or inconsistent CSR arrays  */
+#define MG_E_OOM      -3   /* device or host allocation failed / over budget  */
+#define MG_E_CAPACITY -4   /* emit output truncated at cap_rows               */
+#define MG_E_TIMEOUT  -5   /* a bounded device wait expired                   */
+#define MG_E_CUDA     -6   /* CUDA runtime error                              */
+#define MG_E_ARG      -7   /* invalid argument                                */
+#define MG_E_LIMIT    -8   /* input beyond a documented engine limit          */
+
+#define MG_MAX_QUERY_VERTICES 16   /* k <= 16                                */
+#define MG_MAX_LABELS        256   /* distinct vertex labels in a data graph  */
+
+/* ---- CSR view: the reference's binary CSR directory, in memory ---------- *
+ * Layout of graphs/0.bin (uint32 arrays, in this order) — replaces the
+ * buffers parsed by ImmutableCSR::Read / ParseBasePtr
+ * (core/data_structures/immutable_csr.cu:79-101, :168-247):
+ *   globalid[n] indeg[n] outdeg[n] in_off[n+1] out_off[n+1]
+ *   in_edges[m_in] out_edges[m_out]
+ *   edges_globalid_by_localid[max_vid+1] localid_by_globalid[max_vid+1]
+ * label/0.bin holds labels[n].  Adjacency entries are GLOBAL vertex ids
+ * (core/util/format_converter.cuh:166-184).  All pointers are host memory
+ * owned by the caller (or by the owner handle of mg_csr_dir_open).
+ * edges_globalid_by_localid / localid_by_globalid may be NULL.          */
+typedef struct mg_csr_view {
+  uint32_t n;          /* num_vertices                                      */
+  uint32_t max_vid;
+  uint32_t min_vid;
+  uint32_t m_in;       /* num_incoming_edges                                */
+  uint32_t m_out;      /* num_outgoing_edges                                */
+  uint32_t _pad;
+  const uint32_t* globalid;
+  const uint32_t* indeg;
+  const uint32_t* outdeg;
+  const uint32_t* in_off;
+  const uint32_t* out_off;
+  const uint32_t* in_edges;
+  const uint32_t* out_edges;
+  const uint32_t* edges_globalid_by_localid;
+  const uint32_t* localid_by_globalid;
+  const uint32_t* labels;
+} mg_csr_view;
+
+/* Matching order selection. */
+#define MG_ORDER_REFERENCE 0  /* vertex-introduction order of the reference WOJ
+                                 edge chain (core/data_structures/
+                                 woj_exec_plan.cuh:36-45), rescanning skipped
+                                 edges so every vertex is placed            */
+#define MG_ORDER_STRONG    1  /* fewest candidates first, then most backward
+                                 neighbours                                  */
+#define MG_ORDER_LEARNED   2  /* order chosen by a loaded order model        */
+#define MG_ORDER_GIVEN     3  /* opts->given_order[k] (query local ids)      */
+
+/* Candidate-filter bits (all sound: they never remove a true match). */
+#define MG_FILTER_DEGREE 1u   /* deg(v) >= deg_q(u): kernel_woj_subsio.cu:123-138 */
+#define MG_FILTER_NLB    2u   /* neighbour-label bit subset: the sound form of
+                                 NeighborLabelCounterFilter :385-446          */
+#define MG_FILTER_ALL    3u
+
+typedef struct mg_opts {
+  int32_t  order;            /* MG_ORDER_*                                   */
+  uint32_t filters;          /* MG_FILTER_* bits; default MG_FILTER_ALL      */
+  const uint32_t* given_order; /* k query-local ids when order == GIVEN      */
+  void*    model;            /* order model for MG_ORDER_LEARNED (may be NULL:
+                                then the reference order is used)            */
+  uint64_t chunk_rows;       /* partial-match rows per level chunk; 0 = auto */
+  uint32_t block;            /* threads per block of the expand kernel; 0=auto */
+  uint32_t merge_min;        /* warp-merge intersection when the other list's
+                                covered window <= merge_min*32; 0 = auto     */
+  uint32_t spin_limit;       /* iteration cap of device waits; 0 = default   */
+  uint32_t persistent;       /* 1: one persistent launch drives all levels  */
+  uint64_t mem_budget_bytes; /* cap on enumeration scratch; 0 = auto        */
+  uint64_t root_begin;       /* level-0 candidates [root_begin, root_end) of  */
+  uint64_t root_end;         /* the first position's label bucket; 0,0 = all  */
+} mg_opts;
+
+/* Per-call statistics (optional out-parameter of the *_ex entry points). */
+typedef struct mg_stats {
+  uint32_t k;
+  uint32_t order[MG_MAX_QUERY_VERTICES];        /* chosen order (query ids) */
+  uint64_t level_rows[MG_MAX_QUERY_VERTICES + 1]; /* P_i: surviving prefixes of
+                                                   length i (i = 1..k)       */
+  uint64_t balg_bytes;       /* algorithmic bytes, full-slice definition     */
+  uint64_t balg_count_bytes; /* algorithmic bytes, count-mode definition     */
+  double   device_ms;        /* device time from first launch to result      */
+  uint64_t launches;         /* kernels launched by this call                */
+  uint64_t chunks;           /* level chunks processed                       */
+} mg_stats;
+
+typedef struct mg_graph_info {
+  uint32_t n;
+  uint32_t n_labels;         /* distinct labels after compaction             */
+  uint64_t m_out;            /* distinct directed adjacency entries (out)    */
+  uint64_t m_in;
+  uint32_t symmetric;        /* 1 if in-CSR == out-CSR                       */
+  uint32_t device;
+  uint64_t device_bytes;     /* resident bytes of graph + derived indices    */
+  uint32_t max_degree;
+  uint32_t nlb_words;        /* W = ceil(n_labels / 32)                       */
+} mg_graph_info;
+
+/* ---- library ------------------------------------------------------------ */
+const char* mg_last_error(void);
+const char* mg_version(void);
+void mg_opts_default(mg_opts* o);
+
+/* ---- reference CSR directory format ------------------------------------- */
+/* Replaces ImmutableCSR::Read (core/data_structures/immutable_csr.cu:168-247)
+ * and the meta.yaml decoder (core/common/yaml_config.h:85-110).  `dir` is a
+ * directory prefix that ends in '/', exactly as the reference concatenates
+ * it.  *owner receives the host memory holding the arrays.               */
+int  mg_csr_dir_open(const char* dir, mg_csr_view* out, void** owner);
+void mg_csr_dir_close(void* owner);
+/* Replaces ImmutableCSR::Write (core/data_structures/immutable_csr.cu:103-166);
+ * num_edges = m_in + m_out wraps modulo 2^32 as the reference's uint32 sum. */
+int  mg_csr_dir_write(const char* dir, const mg_csr_view* g);
+
+/* Build a reference-layout CSR from a directed edge list (host).  Replaces
+ * Edgelist2ImmutableCSR (core/util/format_converter.cuh:91-284): vertex ids
+ * 0..n-1, per-vertex sorted adjacency, labels given.  flags bit0: add the
+ * reverse of every edge; bit1: drop self-loops; bit2: drop duplicates.     */
+#define MG_BUILD_SYMMETRIZE 1u
+#define MG_BUILD_NO_SELF    2u
+#define MG_BUILD_DEDUP      4u
+int  mg_csr_from_edges(uint32_t n, const uint32_t* src, const uint32_t* dst,
+                       uint64_t m, const uint32_t* labels, uint32_t flags,
+                       mg_csr_view* out, void** owner);
+/* Edge list CSV ("src,dst" per line) -> CSR with first-appearance id
+ * compaction and labels vid % label_range.  Replaces
+ * ConvertEdgelistCSV2ImmutableCSR (tools/graph_converter/
+ * to_immutable_csr.cuh:21-73) with Edges::ReadFromCSV
+ * (core/data_structures/edgelist.cu:200-290) and GenerateVLabel
+ * (core/data_structures/edgelist.cu:425).                                 */
+int  mg_csr_from_csv(const char* csv_path, uint32_t label_range,
+                     mg_csr_view* out, void** owner);
+
+/* ---- synthetic inputs (seeded, counter-based Philox4x32-10) ------------- */
+/* Chung-Lu power-law graph: weights c*(i+1)^(-1/(beta-1)) scaled so that
+ * sum(w) = n*avg_deg; every pair i<j included with p = min(1, wi*wj/sum w);
+ * symmetrised, no self-loops, sorted adjacency.                            */
+int  mg_gen_chung_lu(uint32_t n, double beta, double avg_deg, uint64_t seed,
+                     uint32_t threads, uint32_t** src, uint32_t** dst,
+                     uint64_t* m);
+/* R-MAT: 2^scale vertices, edge_factor*2^scale directed draws with
+ * quadrant probabilities (a, b, c, 1-a-b-c), `scale` levels per edge.     */
+int  mg_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b,
+                 double c, uint64_t seed, uint32_t threads, uint32_t** src,
+                 uint32_t** dst, uint64_t* m);
+void mg_free_buffer(void* p);
+/* Vertex labels: kind 0 uniform over L, kind 1 Zipf P(k) ~ (k+1)^-s.     */
+int  mg_gen_labels(uint32_t n, uint32_t kind, uint32_t L, double s,
+                   uint64_t seed, uint32_t* labels);
+/* Labelled query from a shape given as an undirected edge list over k
+ * vertices; labels copied from a random walk on the data graph along the
+ * query's BFS spanning tree from vertex 0.  The query is symmetrised.     */
+int  mg_gen_query_walk(const mg_csr_view* g, uint32_t k, const uint32_t* eu,
+                       const uint32_t* ev, uint32_t ne, uint64_t seed,
+                       mg_csr_view* out, void** owner);
+/* Random connected query: recursive spanning tree (vertex j joins a uniform
+ * earlier vertex) plus every other pair with probability p_extra, labels by
+ * random walk.                                                             */
+int  mg_gen_query_random(const mg_csr_view* g, uint32_t k, double p_extra,
+                         uint64_t seed, mg_csr_view* out, void** owner);
+/* Query with explicit labels from an undirected edge list (symmetrised). */
+int  mg_query_from_edges(uint32_t k, const uint32_t* eu, const uint32_t* ev,
+                         uint32_t ne, const uint32_t* labels, int directed,
+                         mg_csr_view* out, void** owner);
+
+/* ---- matching plan ------------------------------------------------------ */
+/* Replaces WOJExecutionPlan::GenerateWOJExecutionPlan
+ * (core/data_structures/woj_exec_plan.cuh:33-50): writes the matching
+ * order (k query-local ids) for the given graph, query and options.
+ * dgraph may be NULL for MG_ORDER_REFERENCE and MG_ORDER_GIVEN.           */
+int  mg_plan_order(void* dgraph, const mg_csr_view* q, const mg_opts* opts,
+                   uint32_t* order, uint32_t* k);
+
+/* ---- device graph ------------------------------------------------------- */
+/* Uploads a data graph to `device` and builds the derived indices
+ * (label-sliced adjacency, neighbour-label bits, label buckets).  Replaces
+ * the UnifiedOwnedBuffer::Init uploads of WOJSubIsoKernelWrapper::Filter
+ * (core/task/gpu_task/kernel/kernel_woj_subsio.cu:753-815).               */
+int  mg_graph_upload(const mg_csr_view* g, int device, void** dgraph);
+void mg_graph_free(void* dgraph);
+int  mg_graph_get_info(void* dgraph, mg_graph_info* info);
+
+/* ---- matching ----------------------------------------------------------- */
+/* Exact match count.  Replaces WOJSubIsoKernelWrapper::Filter + ::Join
+ * (core/task/gpu_task/kernel/kernel_woj_subiso.cuh:45-51,
+ * kernel_woj_subsio.cu:723-1079) as called by SubIso::WOJMatching
+ * (core/task/gpu_task/subiso.cu:201-234).                                  */
+int  mg_subiso_count(void* dgraph, const mg_csr_view* q, const mg_opts* opts,
+                     uint64_t* count);
+int  mg_subiso_count_ex(void* dgraph, const mg_csr_view* q,
+                        const mg_opts* opts, uint64_t* count, mg_stats* st);
+/* All matches as rows of k GLOBAL data-vertex ids in query-local-id order,
+ * sorted lexicographically.  *n_rows receives the full count; when it
+ * exceeds cap_rows, the first cap_rows rows in sorted order are written and
+ * MG_E_CAPACITY is returned.  Replaces the join output tables
+ * (core/data_structures/woj_matches.cuh:15-98) printed by
+ * WOJMatches::Print (core/data_structures/woj_matches.cu:140).           */
+int  mg_subiso_emit(void* dgraph, const mg_csr_view* q, const mg_opts* opts,
+                    uint32_t* rows, uint64_t cap_rows, uint64_t* n_rows);
+int  mg_subiso_emit_ex(void* dgraph, const mg_csr_view* q,
+                       const mg_opts* opts, uint32_t* rows, uint64_t cap_rows,
+                       uint64_t* n_rows, mg_stats* st);
+/* Counts for nq queries in one batch against one resident data graph.
+ * Replaces nq calls of SubIso::Run (core/task/gpu_task/subiso.cu:236-260). */
+int  mg_subiso_batch_count(void* dgraph, const mg_csr_view* const* qs,
+                           uint32_t nq, const mg_opts* opts, uint64_t* counts);
+int  mg_subiso_batch_count_ex(void* dgraph, const mg_csr_view* const* qs,
+                              uint32_t nq, const mg_opts* opts,
+                              uint64_t* counts, mg_stats* st);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MG_SUBISO_H_ */

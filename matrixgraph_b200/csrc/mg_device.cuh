@@ -1,0 +1,94 @@
+// Device-side data layout of a resident data graph and of matching plans.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <memory>
+
+#include "mg_internal.h"
+
+namespace mg {
+
+constexpr int MAXK = MG_MAX_QUERY_VERTICES;
+constexpr int WMAX = MG_MAX_LABELS / 32;
+constexpr uint8_t DCI_BUCKET = 0xFF;
+constexpr uint32_t FULL = 0xFFFFFFFFu;
+
+// Error bits raised by kernels (read back by the host after each call).
+constexpr uint32_t ERR_OVERFLOW = 1u;   // a table write exceeded its capacity
+constexpr uint32_t ERR_RANGE = 2u;      // an adjacency id outside [0, n)
+constexpr uint32_t ERR_TIMEOUT = 4u;    // a bounded device wait gave up
+
+// Read-only view of a resident graph, passed by value to kernels.
+//   adj[d]   : adjacency of direction d (0 = out, 1 = in), each vertex's list
+//              ordered by (label, id): label slices are contiguous and sorted
+//   loff[d]  : n*L+1 slice starts; slice (v, l) = [loff[v*L+l], loff[v*L+l+1])
+//   nlb[d]   : n*W neighbour-label bits (bit l: v has a d-neighbour labelled l)
+//   deg[d]   : distinct d-neighbours
+//   label    : compact labels 0..L-1
+//   bucket_* : vertices grouped by label (ascending id inside a bucket)
+//   selfbits : bit v set when (v, v) is an edge
+//   globalid : local id -> global id of the reference format
+struct GraphDev {
+  uint32_t n, L, W, symmetric;
+  const uint32_t* adj[2];
+  const uint32_t* loff[2];
+  const uint32_t* nlb[2];
+  const uint32_t* deg[2];
+  const uint32_t* label;
+  const uint32_t* bucket_off;
+  const uint32_t* bucket_vid;
+  const uint32_t* selfbits;
+  const uint32_t* globalid;
+};
+
+// Matching plan of one query for one order.  Position i matches query vertex
+// perm[i].  cons[i][c] = pos | dir << 8: the candidate for position i must be
+// in the dir-adjacency of the vertex matched at position pos (< i).
+struct PlanDev {
+  uint32_t k;
+  uint32_t last_o1;         // last position has one constraint, no self-loop
+  uint32_t selfloop_mask;   // bit i: query vertex perm[i] has a self-loop
+  uint32_t zero;            // 1: some label of the query is absent (count 0)
+  uint32_t label[MAXK];
+  uint32_t ncons[MAXK];
+  uint32_t cons[MAXK][MAXK];
+  uint32_t req[2][MAXK];               // degree requirement per direction
+  uint32_t nlbq[2][MAXK][WMAX];        // required neighbour-label bits
+  uint32_t samelab[MAXK];              // positions j < i with the same label
+  uint32_t guar[MAXK];                 // last position: m(j) surely in slice
+  uint32_t perm[MAXK];
+};
+
+struct Workspace;  // enumeration scratch (mg_enum.cu)
+
+// Host object behind the opaque dgraph handle.
+struct DevGraph {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  GraphDev g{};
+  mg_graph_info info{};
+  GraphStats stats;
+  bool stats_full = false;   // degree / label-pair statistics computed
+  std::vector<uint32_t> h_bucket_off;
+  std::vector<void*> allocs;
+  Workspace* ws = nullptr;
+  std::mutex mu;
+  ~DevGraph();
+};
+
+int ensure_full_stats(DevGraph* dg);
+
+#define MG_CK(call)                                                          \
+  do {                                                                       \
+    cudaError_t _e = (call);                                                 \
+    if (_e != cudaSuccess)                                                   \
+      return ::mg::set_error(MG_E_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, \
+                             #call, cudaGetErrorString(_e));                 \
+  } while (0)
+
+// cudaMalloc that records the allocation on the graph and maps failure to
+// MG_E_OOM.
+int dev_alloc(DevGraph* dg, void** p, size_t bytes);
+
+}  // namespace mg

@@ -1,0 +1,1076 @@
+// Exact subgraph enumeration: candidate filtering + worst-case-optimal-join
+// extension by sorted-list intersection, as a memory-bounded hybrid
+// BFS/DFS over level tables.
+//
+// Replaces the reference GPU WOJ path (WOJFilterVCKernel
+// core/task/gpu_task/kernel/kernel_woj_subsio.cu:532-604, the per-table
+// MergeSort core/task/gpu_task/kernel/algorithms/sort.cuh:59-105 and
+// WOJJoinKernel kernel_woj_subsio.cu:623-721), which joins one key column at
+// a time, never checks cycle closure or injectivity and caps its output at
+// kMaxNumWeft rows.  Here:
+//   * a level table holds partial matches of prefix length i (SoA columns);
+//   * the work kernel picks, per row, the shortest label slice among the
+//     backward neighbours' adjacency (the driving list) and the scan turns
+//     the driving lengths into an element index space;
+//   * the expand kernel assigns one element (row, driving entry) per thread,
+//     so hub rows spread over many warps; the other backward slices are
+//     probed by binary search, injectivity is checked against the row, the
+//     label/degree/neighbour-label filter prunes, and survivors are appended
+//     with warp-aggregated atomics (__ballot_sync / __popc);
+//   * a table chunk never holds more than `cap` rows: the host walks the
+//     levels depth-first, expanding at most `cap` elements of a level before
+//     descending, so intermediate results never exceed the scratch budget;
+//   * in count mode the last position is never materialised: when it has a
+//     single backward neighbour its count is the slice length minus the
+//     injectivity collisions, added while expanding the position before it.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include <cub/cub.cuh>
+
+#include "mg_device.cuh"
+
+namespace mg {
+
+const char* last_error_cstr();
+
+// ---------------------------------------------------------------------------
+// Workspace (per graph handle)
+// ---------------------------------------------------------------------------
+struct Workspace {
+  int device = 0;
+  uint64_t cap = 0;       // rows per level table (and elements per chunk)
+  uint32_t rows0 = 0;     // capacity of the level-0 table (one row per query)
+  int levels = 0;         // level tables allocated: 0..levels-1
+  uint32_t* col[MAXK][MAXK] = {};
+  uint32_t* qid[MAXK] = {};
+  uint32_t* work[MAXK] = {};
+  uint64_t* woff[MAXK] = {};
+  uint32_t* dstart[MAXK] = {};
+  uint8_t* dci[MAXK] = {};
+  uint64_t* bsum = nullptr;
+  uint32_t bsum_cap = 0;
+  unsigned long long* ctr = nullptr;     // device counters
+  unsigned long long* h_ctr = nullptr;   // pinned mirror
+  unsigned long long* counts = nullptr;  // per query
+  uint32_t counts_cap = 0;
+  PlanDev* plans = nullptr;
+  uint32_t plans_cap = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<void*> allocs;
+  uint64_t bytes = 0;
+};
+
+// Counter slots.
+enum : int { C_OUT = 0, C_BALG = 1, C_BALGC = 2, C_ERR = 3, C_EMIT = 4, C_SURV = 8, C_NUM = 8 + MAXK + 2 };
+
+void free_workspace(Workspace* ws) {
+  if (!ws) return;
+  for (void* p : ws->allocs) cudaFree(p);
+  if (ws->h_ctr) cudaFreeHost(ws->h_ctr);
+  if (ws->ev0) cudaEventDestroy(ws->ev0);
+  if (ws->ev1) cudaEventDestroy(ws->ev1);
+  delete ws;
+}
+
+static int ws_alloc(Workspace* ws, void** p, size_t bytes) {
+  *p = nullptr;
+  cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return set_error(MG_E_OOM, "enumeration scratch: cudaMalloc(%zu) failed: %s", bytes,
+                     cudaGetErrorString(e));
+  }
+  ws->allocs.push_back(*p);
+  ws->bytes += bytes;
+  return MG_OK;
+}
+
+constexpr uint64_t kDefaultCap = 1ull << 24;
+constexpr int SCAN_TILE = 4096;
+
+static uint64_t level_row_bytes(int l) { return uint64_t(l) * 4 + 4 + 4 + 8 + 4 + 1; }
+
+static int ensure_ws(DevGraph* dg, uint64_t cap, int levels, uint32_t nq) {
+  Workspace*& ws = dg->ws;
+  if (ws && (ws->cap != cap || ws->rows0 < nq)) {
+    cudaStreamSynchronize(dg->stream);
+    free_workspace(ws);
+    ws = nullptr;
+  }
+  if (!ws) {
+    ws = new Workspace();
+    ws->device = dg->device;
+    ws->cap = cap;
+    ws->rows0 = std::max<uint32_t>(nq, 1024);
+    int rc;
+    if ((rc = ws_alloc(ws, (void**)&ws->ctr, C_NUM * 8))) return rc;
+    MG_CK(cudaMallocHost((void**)&ws->h_ctr, C_NUM * 8));
+    MG_CK(cudaEventCreate(&ws->ev0));
+    MG_CK(cudaEventCreate(&ws->ev1));
+    ws->bsum_cap = uint32_t((std::max<uint64_t>(cap, ws->rows0) + SCAN_TILE - 1) / SCAN_TILE + 1);
+    if ((rc = ws_alloc(ws, (void**)&ws->bsum, uint64_t(ws->bsum_cap) * 8))) return rc;
+  }
+  if (ws->counts_cap < nq) {
+    int rc;
+    if ((rc = ws_alloc(ws, (void**)&ws->counts, uint64_t(nq) * 8))) return rc;
+    if ((rc = ws_alloc(ws, (void**)&ws->plans, uint64_t(nq) * sizeof(PlanDev)))) return rc;
+    ws->counts_cap = ws->plans_cap = nq;
+  }
+  for (int l = ws->levels; l < levels; ++l) {
+    const uint64_t rows = l == 0 ? ws->rows0 : cap;
+    int rc;
+    for (int j = 0; j < l; ++j)
+      if ((rc = ws_alloc(ws, (void**)&ws->col[l][j], rows * 4))) return rc;
+    if ((rc = ws_alloc(ws, (void**)&ws->qid[l], rows * 4))) return rc;
+    if ((rc = ws_alloc(ws, (void**)&ws->work[l], rows * 4))) return rc;
+    if ((rc = ws_alloc(ws, (void**)&ws->woff[l], (rows + 1) * 8))) return rc;
+    if ((rc = ws_alloc(ws, (void**)&ws->dstart[l], rows * 4))) return rc;
+    if ((rc = ws_alloc(ws, (void**)&ws->dci[l], rows))) return rc;
+    ws->levels = l + 1;
+  }
+  return MG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+struct TabPtrs {
+  uint32_t* col[MAXK];
+  uint32_t* qid;  // nullptr: single query, q = 0
+};
+
+struct StepArgs {
+  GraphDev g;
+  const PlanDev* plans;
+  uint32_t level;   // rows hold positions 0..level-1; position `level` is extended
+  uint32_t R;       // rows of the input table
+  TabPtrs in;
+  uint32_t* work;
+  uint64_t* woff;
+  uint32_t* dstart;
+  uint8_t* dci;
+  uint64_t t0, t1;  // element range of this expand launch
+  TabPtrs out;
+  uint64_t out_cap;
+  unsigned long long* ctr;
+  unsigned long long* counts;
+  uint32_t count_mode;
+  uint32_t filters;
+  uint32_t stats;
+  uint32_t nq;
+  uint32_t* emit_col[MAXK];
+  uint64_t emit_cap;
+  uint64_t root_begin, root_end;  // level-0 candidate range (root_end 0: all)
+};
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t l = threadIdx.x & 31;
+  return (1u << l) - 1u;
+}
+
+// Binary search for x in the sorted range a[s, e).
+__device__ __forceinline__ bool contains(const uint32_t* __restrict__ a, uint32_t s, uint32_t e,
+                                         uint32_t x) {
+  uint32_t lo = s, hi = e;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    uint32_t v = __ldg(a + mid);
+    if (v < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo < e && __ldg(a + lo) == x;
+}
+
+__device__ __forceinline__ void slice_of(const GraphDev& g, uint32_t dir, uint32_t y,
+                                         uint32_t lab, uint32_t& s, uint32_t& e) {
+  const uint32_t* p = g.loff[dir] + uint64_t(y) * g.L + lab;
+  s = __ldg(p);
+  e = __ldg(p + 1);
+}
+
+__device__ __forceinline__ bool pass_filters(const GraphDev& g, const PlanDev& P, uint32_t i,
+                                             uint32_t x, uint32_t filters) {
+  if (filters & MG_FILTER_DEGREE) {
+    if (__ldg(g.deg[0] + x) < P.req[0][i]) return false;
+    if (!g.symmetric && __ldg(g.deg[1] + x) < P.req[1][i]) return false;
+  }
+  if (filters & MG_FILTER_NLB) {
+    for (uint32_t w = 0; w < g.W; ++w) {
+      if (P.nlbq[0][i][w] & ~__ldg(g.nlb[0] + uint64_t(x) * g.W + w)) return false;
+      if (!g.symmetric && (P.nlbq[1][i][w] & ~__ldg(g.nlb[1] + uint64_t(x) * g.W + w)))
+        return false;
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ bool has_self(const GraphDev& g, uint32_t x) {
+  return (__ldg(g.selfbits + (x >> 5)) >> (x & 31)) & 1u;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+  for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(FULL, v, d);
+  return v;
+}
+
+// Largest r in [lo, hi] with woff[r] <= t (woff non-decreasing, woff[lo] <= t).
+__device__ __forceinline__ uint32_t find_row(const uint64_t* __restrict__ woff, uint32_t lo,
+                                             uint32_t hi, uint64_t t) {
+  while (lo < hi) {
+    uint32_t mid = (lo + hi + 1) >> 1;
+    if (woff[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Work kernel: per row, the driving slice (shortest backward slice, or the
+// label bucket for a position without backward neighbours) and the
+// algorithmic-byte charge of extending the row.
+__global__ void __launch_bounds__(256) k_work(StepArgs a) {
+  unsigned long long bal = 0, balc = 0;
+  const uint32_t i = a.level;
+  const GraphDev& g = a.g;
+  for (uint64_t r = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; r < a.R;
+       r += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t q = a.in.qid ? a.in.qid[r] : 0u;
+    const PlanDev& P = a.plans[q];
+    const uint32_t lab = P.label[i];
+    const uint32_t nc = P.ncons[i];
+    uint32_t best, bs = 0;
+    uint8_t bci = DCI_BUCKET;
+    unsigned long long ch = 0, chc = 0;
+    if (P.zero) {
+      best = 0;
+    } else if (nc == 0) {
+      bs = __ldg(g.bucket_off + lab);
+      best = __ldg(g.bucket_off + lab + 1) - bs;
+      if (i == 0 && a.root_end) {
+        const uint64_t rb = a.root_begin < best ? a.root_begin : uint64_t(best);
+        const uint64_t re = a.root_end < best ? a.root_end : uint64_t(best);
+        bs += uint32_t(rb);
+        best = re > rb ? uint32_t(re - rb) : 0u;
+      }
+      ch = chc = (unsigned long long)best * (12ull + 4ull * g.W);
+    } else {
+      best = FULL;
+      for (uint32_t c = 0; c < nc; ++c) {
+        const uint32_t cs = P.cons[i][c];
+        const uint32_t y = a.in.col[cs & 0xFF][r];
+        uint32_t s, e;
+        slice_of(g, cs >> 8, y, lab, s, e);
+        ch += 8ull + 4ull * (e - s);
+        if (e - s < best) {
+          best = e - s;
+          bs = s;
+          bci = uint8_t(c);
+        }
+      }
+      chc = (i + 1 == P.k && P.last_o1) ? 8ull : ch;
+    }
+    a.work[r] = best;
+    a.dstart[r] = bs;
+    a.dci[r] = bci;
+    bal += ch;
+    balc += chc;
+  }
+  bal = warp_sum(bal);
+  balc = warp_sum(balc);
+  if ((threadIdx.x & 31) == 0 && (bal | balc)) {
+    atomicAdd(&a.ctr[C_BALG], bal);
+    atomicAdd(&a.ctr[C_BALGC], balc);
+  }
+}
+
+// Scan of the per-row driving lengths into 64-bit element offsets.
+__device__ __forceinline__ unsigned long long block_exclusive_scan(unsigned long long v,
+                                                                   unsigned long long* total) {
+  __shared__ unsigned long long wsum[33];
+  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned long long incl = v;
+  for (int d = 1; d < 32; d <<= 1) {
+    unsigned long long t = __shfl_up_sync(FULL, incl, d);
+    if (lane >= d) incl += t;
+  }
+  if (lane == 31) wsum[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    const uint32_t nw = blockDim.x >> 5;
+    unsigned long long s = lane < nw ? wsum[lane] : 0ull;
+    unsigned long long si = s;
+    for (int d = 1; d < 32; d <<= 1) {
+      unsigned long long t = __shfl_up_sync(FULL, si, d);
+      if (lane >= d) si += t;
+    }
+    if (lane < nw) wsum[lane] = si - s;
+    if (lane == nw - 1) wsum[32] = si;
+  }
+  __syncthreads();
+  unsigned long long res = wsum[wid] + incl - v;
+  *total = wsum[32];
+  __syncthreads();
+  return res;
+}
+
+__global__ void __launch_bounds__(256) k_scan_reduce(const uint32_t* __restrict__ in, uint32_t R,
+                                                     uint64_t* bsum) {
+  const uint64_t base = uint64_t(blockIdx.x) * SCAN_TILE;
+  unsigned long long s = 0;
+  for (uint32_t j = threadIdx.x; j < SCAN_TILE; j += blockDim.x) {
+    uint64_t idx = base + j;
+    if (idx < R) s += in[idx];
+  }
+  s = warp_sum(s);
+  __shared__ unsigned long long ws[8];
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) t += ws[w];
+    bsum[blockIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_scan_bsum(uint64_t* bsum, uint32_t nb, uint64_t* total_out) {
+  __shared__ unsigned long long carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t base = 0; base < nb; base += blockDim.x) {
+    uint32_t i = base + threadIdx.x;
+    unsigned long long v = i < nb ? bsum[i] : 0ull;
+    unsigned long long tot;
+    unsigned long long ex = block_exclusive_scan(v, &tot);
+    if (i < nb) bsum[i] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total_out = carry;
+}
+
+__global__ void __launch_bounds__(256) k_scan_apply(const uint32_t* __restrict__ in, uint32_t R,
+                                                    const uint64_t* __restrict__ bsum,
+                                                    uint64_t* out) {
+  __shared__ uint32_t tile[SCAN_TILE + SCAN_TILE / 32];
+  const uint64_t base = uint64_t(blockIdx.x) * SCAN_TILE;
+  for (uint32_t j = threadIdx.x; j < SCAN_TILE; j += blockDim.x) {
+    uint64_t idx = base + j;
+    tile[j + (j >> 5)] = idx < R ? in[idx] : 0u;
+  }
+  __syncthreads();
+  constexpr uint32_t PER = SCAN_TILE / 256;
+  const uint32_t t0 = threadIdx.x * PER;
+  unsigned long long s = 0;
+  for (uint32_t j = 0; j < PER; ++j) s += tile[(t0 + j) + ((t0 + j) >> 5)];
+  unsigned long long tot;
+  unsigned long long ex = block_exclusive_scan(s, &tot) + bsum[blockIdx.x];
+  for (uint32_t j = 0; j < PER; ++j) {
+    uint64_t idx = base + t0 + j;
+    if (idx < R) out[idx] = ex;
+    ex += tile[(t0 + j) + ((t0 + j) >> 5)];
+  }
+}
+
+// Expand kernel: one element (row, driving entry) per thread.
+constexpr int EXPAND_BLOCK = 256;
+
+__global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
+  __shared__ uint32_t s_rlo, s_rhi;
+  const uint32_t i = a.level;
+  const GraphDev& g = a.g;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t span = a.t1 - a.t0;
+  const uint64_t ntiles = (span + EXPAND_BLOCK - 1) / EXPAND_BLOCK;
+  unsigned long long cnt = 0, bal = 0, balc = 0, surv1 = 0, survk = 0;
+  uint32_t cnt_q = 0;
+  for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const uint64_t tb = a.t0 + tile * EXPAND_BLOCK;
+    const uint64_t te = min(tb + EXPAND_BLOCK, a.t1);
+    if (threadIdx.x == 0) s_rlo = find_row(a.woff, 0, a.R - 1, tb);
+    if (threadIdx.x == 32) s_rhi = find_row(a.woff, 0, a.R - 1, te - 1);
+    __syncthreads();
+    const uint32_t rlo = s_rlo, rhi = s_rhi;
+    __syncthreads();
+    const uint64_t t = tb + threadIdx.x;
+    const bool valid = t < te;
+    bool ok = false, fin = false, fused = false;
+    uint32_t r = 0, x = 0, q = 0;
+    if (valid) {
+      r = find_row(a.woff, rlo, rhi, t);
+      const uint32_t e = uint32_t(t - a.woff[r]);
+      const uint8_t ci = a.dci[r];
+      const uint32_t ds = a.dstart[r];
+      q = a.in.qid ? a.in.qid[r] : 0u;
+      const PlanDev& P = a.plans[q];
+      const uint32_t lab = P.label[i];
+      uint32_t ddir = 0;
+      if (ci == DCI_BUCKET) {
+        x = __ldg(g.bucket_vid + ds + e);
+      } else {
+        ddir = P.cons[i][ci] >> 8;
+        x = __ldg(g.adj[ddir] + ds + e);
+      }
+      ok = true;
+      // injectivity: only earlier positions with the same label can collide
+      for (uint32_t m = P.samelab[i]; m && ok; m &= m - 1) {
+        const uint32_t j = __ffs(m) - 1;
+        if (a.in.col[j][r] == x) ok = false;
+      }
+      // remaining backward neighbours: binary search in their label slices
+      const uint32_t nc = P.ncons[i];
+      for (uint32_t c = 0; c < nc && ok; ++c) {
+        if (c == ci) continue;
+        const uint32_t cs = P.cons[i][c];
+        const uint32_t y = a.in.col[cs & 0xFF][r];
+        uint32_t s, en;
+        slice_of(g, cs >> 8, y, lab, s, en);
+        ok = contains(g.adj[cs >> 8], s, en, x);
+      }
+      if (ok && ((P.selfloop_mask >> i) & 1u)) ok = has_self(g, x);
+      fin = (i + 1 == P.k);
+      fused = !fin && a.count_mode && (i + 2 == P.k) && P.last_o1;
+      if (ok && !fin && a.filters) ok = pass_filters(g, P, i, x, a.filters);
+      if (ok) {
+        surv1 += 1;
+        if (fin) {
+          if (a.count_mode) {
+            if (q != cnt_q) {
+              if (cnt) atomicAdd(&a.counts[cnt_q], cnt);
+              cnt = 0;
+              cnt_q = q;
+            }
+            cnt += 1;
+          }
+        } else if (fused) {
+          const uint32_t kl = P.k - 1;
+          const uint32_t cs = P.cons[kl][0];
+          const uint32_t pos = cs & 0xFF, dir = cs >> 8;
+          const uint32_t y = pos == i ? x : a.in.col[pos][r];
+          uint32_t s, en;
+          slice_of(g, dir, y, P.label[kl], s, en);
+          unsigned long long c1 = en - s;
+          bal += 8ull + 4ull * c1;
+          balc += 8ull;
+          for (uint32_t m = P.samelab[kl]; m; m &= m - 1) {
+            const uint32_t j = __ffs(m) - 1;
+            if ((P.guar[kl] >> j) & 1u) {
+              c1 -= 1;
+            } else {
+              const uint32_t mj = j == i ? x : a.in.col[j][r];
+              c1 -= contains(g.adj[dir], s, en, mj) ? 1ull : 0ull;
+            }
+          }
+          survk += c1;
+          if (q != cnt_q) {
+            if (cnt) atomicAdd(&a.counts[cnt_q], cnt);
+            cnt = 0;
+            cnt_q = q;
+          }
+          cnt += c1;
+        }
+      }
+    }
+    // Survivors that extend the prefix: append to the next level table.
+    const bool wr = ok && !fin && !fused;
+    const uint32_t wm = __ballot_sync(FULL, wr);
+    if (wm) {
+      const uint32_t leader = __ffs(wm) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(&a.ctr[C_OUT], (unsigned long long)__popc(wm));
+      base = __shfl_sync(FULL, base, leader);
+      if (wr) {
+        const unsigned long long idx = base + __popc(wm & lanemask_lt());
+        if (idx < a.out_cap) {
+          for (uint32_t j = 0; j < i; ++j) a.out.col[j][idx] = a.in.col[j][r];
+          a.out.col[i][idx] = x;
+          if (a.out.qid) a.out.qid[idx] = q;
+        } else {
+          atomicOr(&a.ctr[C_ERR], (unsigned long long)ERR_OVERFLOW);
+        }
+      }
+    }
+    // Emit mode: complete matches as rows in query-vertex order.
+    const bool em = ok && fin && !a.count_mode;
+    const uint32_t emm = __ballot_sync(FULL, em);
+    if (emm) {
+      const uint32_t leader = __ffs(emm) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(&a.ctr[C_EMIT], (unsigned long long)__popc(emm));
+      base = __shfl_sync(FULL, base, leader);
+      if (em) {
+        const unsigned long long idx = base + __popc(emm & lanemask_lt());
+        if (idx < a.emit_cap) {
+          const PlanDev& P = a.plans[q];
+          for (uint32_t j = 0; j < i; ++j)
+            a.emit_col[P.perm[j]][idx] = __ldg(g.globalid + a.in.col[j][r]);
+          a.emit_col[P.perm[i]][idx] = __ldg(g.globalid + x);
+        } else {
+          atomicOr(&a.ctr[C_ERR], (unsigned long long)ERR_OVERFLOW);
+        }
+      }
+    }
+  }
+  // Flush per-thread counts: warp-reduce when the whole warp holds one query.
+  const uint32_t same = __match_any_sync(FULL, cnt_q);
+  if (same == FULL) {
+    unsigned long long s = warp_sum(cnt);
+    if (lane == 0 && s) atomicAdd(&a.counts[cnt_q], s);
+  } else if (cnt) {
+    atomicAdd(&a.counts[cnt_q], cnt);
+  }
+  bal = warp_sum(bal);
+  balc = warp_sum(balc);
+  if (lane == 0 && (bal | balc)) {
+    atomicAdd(&a.ctr[C_BALG], bal);
+    atomicAdd(&a.ctr[C_BALGC], balc);
+  }
+  if (a.stats) {
+    surv1 = warp_sum(surv1);
+    survk = warp_sum(survk);
+    if (lane == 0) {
+      if (surv1) atomicAdd(&a.ctr[C_SURV + i + 1], surv1);
+      if (survk) atomicAdd(&a.ctr[C_SURV + a.plans[0].k], survk);
+    }
+  }
+}
+
+__global__ void k_iota(uint32_t* p, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    p[i] = i;
+}
+
+// ---------------------------------------------------------------------------
+// Plans
+// ---------------------------------------------------------------------------
+int build_plan(const DevGraph* dg, const QueryGraph& Q, const uint32_t* order, PlanDev* P) {
+  std::memset(P, 0, sizeof(*P));
+  const uint32_t k = Q.k;
+  P->k = k;
+  const bool sym = dg->g.symmetric != 0;
+  int clab[MAXK];
+  for (uint32_t u = 0; u < k; ++u) clab[u] = dg->stats.compact_label(Q.label_raw[u]);
+  for (uint32_t i = 0; i < k; ++i) {
+    const uint32_t u = order[i];
+    P->perm[i] = u;
+    if (clab[u] < 0) P->zero = 1;
+    P->label[i] = clab[u] < 0 ? 0 : uint32_t(clab[u]);
+  }
+  for (uint32_t i = 0; i < k; ++i) {
+    const uint32_t u = order[i];
+    uint32_t nc = 0;
+    for (uint32_t j = 0; j < i; ++j) {
+      const uint32_t w = order[j];
+      const bool w_to_u = (Q.out_mask[w] >> u) & 1u;  // u in N_out(w)
+      const bool u_to_w = (Q.out_mask[u] >> w) & 1u;  // u in N_in(w)
+      if (sym) {
+        if (w_to_u || u_to_w) P->cons[i][nc++] = j;
+      } else {
+        if (w_to_u) P->cons[i][nc++] = j;
+        if (u_to_w) P->cons[i][nc++] = j | (1u << 8);
+      }
+      if (Q.label_raw[w] == Q.label_raw[u]) P->samelab[i] |= 1u << j;
+    }
+    P->ncons[i] = nc;
+    if ((Q.out_mask[u] >> u) & 1u) P->selfloop_mask |= 1u << i;
+    uint32_t nb0 = sym ? (Q.out_mask[u] | Q.in_mask[u]) : Q.out_mask[u];
+    uint32_t nb1 = Q.in_mask[u];
+    P->req[0][i] = __builtin_popcount(nb0);
+    P->req[1][i] = sym ? 0 : __builtin_popcount(nb1);
+    for (uint32_t w = 0; w < k; ++w) {
+      if (clab[w] < 0) continue;
+      if ((nb0 >> w) & 1u) P->nlbq[0][i][clab[w] >> 5] |= 1u << (clab[w] & 31);
+      if (!sym && ((nb1 >> w) & 1u)) P->nlbq[1][i][clab[w] >> 5] |= 1u << (clab[w] & 31);
+    }
+  }
+  const uint32_t kl = k - 1;
+  P->last_o1 = (k >= 2 && P->ncons[kl] == 1 && !((P->selfloop_mask >> kl) & 1u)) ? 1u : 0u;
+  if (P->last_o1) {
+    const uint32_t cs = P->cons[kl][0];
+    const uint32_t ws = order[cs & 0xFF], dir = cs >> 8;
+    for (uint32_t m = P->samelab[kl]; m; m &= m - 1) {
+      const uint32_t j = __builtin_ctz(m);
+      const uint32_t wj = order[j];
+      bool g;
+      if (sym) g = ((Q.out_mask[ws] >> wj) & 1u) || ((Q.out_mask[wj] >> ws) & 1u);
+      else if (dir == 0) g = (Q.out_mask[ws] >> wj) & 1u;  // m(j) in N_out(m(ws))
+      else g = (Q.out_mask[wj] >> ws) & 1u;                // m(j) in N_in(m(ws))
+      if (g) P->guar[kl] |= 1u << j;
+    }
+  }
+  return MG_OK;
+}
+
+static int choose_order(DevGraph* dg, const QueryGraph& Q, const mg_opts& o, uint32_t* order) {
+  switch (o.order) {
+    case MG_ORDER_REFERENCE:
+      order_reference(Q, order);
+      return MG_OK;
+    case MG_ORDER_STRONG:
+      order_strong(Q, dg->stats, order);
+      return MG_OK;
+    case MG_ORDER_LEARNED: {
+      if (!o.model) {
+        order_reference(Q, order);
+        return MG_OK;
+      }
+      int rc = ensure_full_stats(dg);
+      if (rc) return rc;
+      return order_learned(o.model, Q, dg->stats, order);
+    }
+    case MG_ORDER_GIVEN:
+      if (!o.given_order) return set_error(MG_E_ARG, "MG_ORDER_GIVEN without given_order");
+      std::memcpy(order, o.given_order, Q.k * 4);
+      if (!order_is_permutation(order, Q.k))
+        return set_error(MG_E_ARG, "given_order is not a permutation of 0..%u", Q.k - 1);
+      return MG_OK;
+    default:
+      return set_error(MG_E_ARG, "unknown order %d", o.order);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host driver: depth-first walk over level chunks
+// ---------------------------------------------------------------------------
+struct EmitBuf {
+  uint32_t* col[MAXK] = {};
+  uint64_t cap = 0;
+};
+
+struct RunResult {
+  uint64_t balg = 0, balgc = 0, launches = 0, chunks = 0;
+  uint64_t surv[MAXK + 2] = {};
+  uint64_t emitted = 0;
+  double ms = 0;
+};
+
+static inline unsigned grid_for(uint64_t items, unsigned block, unsigned cap) {
+  uint64_t g = (items + block - 1) / block;
+  return unsigned(std::max<uint64_t>(1, std::min<uint64_t>(g, cap)));
+}
+
+static int run_levels(DevGraph* dg, const std::vector<PlanDev>& plans, bool count_mode,
+                      const EmitBuf* emit, const mg_opts& o, uint64_t* counts_out,
+                      RunResult* res) {
+  const uint32_t nq = uint32_t(plans.size());
+  uint32_t kmax = 1;
+  for (auto& p : plans) kmax = std::max(kmax, p.k);
+  uint64_t cap = o.chunk_rows ? o.chunk_rows : kDefaultCap;
+  cap = std::max<uint64_t>(cap, 1);
+  if (cap > (1ull << 31)) return set_error(MG_E_ARG, "chunk_rows above 2^31");
+  if (o.mem_budget_bytes) {
+    uint64_t per_row = 0;
+    for (uint32_t l = 1; l < kmax; ++l) per_row += level_row_bytes(int(l));
+    if (per_row && cap * per_row > o.mem_budget_bytes) {
+      cap = o.mem_budget_bytes / per_row;
+      if (cap == 0) return set_error(MG_E_OOM, "memory budget below one row per level");
+    }
+  }
+  int rc = ensure_ws(dg, cap, int(kmax), nq);
+  if (rc) return rc;
+  Workspace* ws = dg->ws;
+  cudaStream_t st = dg->stream;
+  MG_CK(cudaMemcpyAsync(ws->plans, plans.data(), nq * sizeof(PlanDev), cudaMemcpyHostToDevice, st));
+  MG_CK(cudaMemsetAsync(ws->counts, 0, nq * 8ull, st));
+  MG_CK(cudaMemsetAsync(ws->ctr, 0, C_NUM * 8, st));
+  MG_CK(cudaEventRecord(ws->ev0, st));
+
+  // writes[l]: some query can append rows to the level-(l+1) table.
+  bool writes[MAXK] = {};
+  for (uint32_t l = 0; l < kmax; ++l)
+    for (auto& p : plans)
+      if (p.k > l + 1 && !(count_mode && p.k == l + 2 && p.last_o1)) writes[l] = true;
+
+  StepArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.g = dg->g;
+  a.plans = ws->plans;
+  a.ctr = ws->ctr;
+  a.counts = ws->counts;
+  a.count_mode = count_mode ? 1u : 0u;
+  a.filters = o.filters & MG_FILTER_ALL;
+  a.stats = nq == 1 ? 1u : 0u;
+  a.nq = nq;
+  if (emit) {
+    for (int j = 0; j < MAXK; ++j) a.emit_col[j] = emit->col[j];
+    a.emit_cap = emit->cap;
+  }
+  if (o.root_end) {
+    if (o.root_begin > o.root_end) return set_error(MG_E_ARG, "root_begin > root_end");
+    a.root_begin = o.root_begin;
+    a.root_end = o.root_end;
+  }
+  const bool batch = nq > 1;
+  if (batch) {
+    k_iota<<<grid_for(nq, 256, 1024), 256, 0, st>>>(ws->qid[0], nq);
+    res->launches++;
+  }
+  uint64_t T[MAXK] = {}, cur[MAXK] = {};
+  uint32_t R[MAXK] = {};
+  R[0] = nq;
+  int lvl = 0;
+  bool need_work = true;
+  const unsigned sms = 148;
+  auto tab = [&](int l) {
+    TabPtrs t{};
+    for (int j = 0; j < l; ++j) t.col[j] = ws->col[l][j];
+    t.qid = batch ? ws->qid[l] : nullptr;
+    return t;
+  };
+  while (true) {
+    if (need_work) {
+      a.level = uint32_t(lvl);
+      a.R = R[lvl];
+      a.in = tab(lvl);
+      a.work = ws->work[lvl];
+      a.woff = ws->woff[lvl];
+      a.dstart = ws->dstart[lvl];
+      a.dci = ws->dci[lvl];
+      k_work<<<grid_for(R[lvl], 256, sms * 16), 256, 0, st>>>(a);
+      const uint32_t nb = (R[lvl] + SCAN_TILE - 1) / SCAN_TILE;
+      k_scan_reduce<<<nb, 256, 0, st>>>(ws->work[lvl], R[lvl], ws->bsum);
+      k_scan_bsum<<<1, 1024, 0, st>>>(ws->bsum, nb, ws->woff[lvl] + R[lvl]);
+      k_scan_apply<<<nb, 256, 0, st>>>(ws->work[lvl], R[lvl], ws->bsum, ws->woff[lvl]);
+      res->launches += 4;
+      MG_CK(cudaMemcpyAsync(&ws->h_ctr[0], ws->woff[lvl] + R[lvl], 8, cudaMemcpyDeviceToHost, st));
+      MG_CK(cudaStreamSynchronize(st));
+      T[lvl] = ws->h_ctr[0];
+      cur[lvl] = 0;
+      need_work = false;
+    }
+    if (cur[lvl] < T[lvl]) {
+      const uint64_t t0 = cur[lvl];
+      const uint64_t t1 = writes[lvl] ? std::min(T[lvl], t0 + cap) : T[lvl];
+      a.level = uint32_t(lvl);
+      a.R = R[lvl];
+      a.in = tab(lvl);
+      a.work = ws->work[lvl];
+      a.woff = ws->woff[lvl];
+      a.dstart = ws->dstart[lvl];
+      a.dci = ws->dci[lvl];
+      a.t0 = t0;
+      a.t1 = t1;
+      if (writes[lvl]) {
+        a.out = tab(lvl + 1);
+        a.out_cap = cap;
+      } else {
+        a.out = TabPtrs{};
+        a.out_cap = 0;
+      }
+      MG_CK(cudaMemsetAsync(ws->ctr + C_OUT, 0, 8, st));
+      const unsigned blocks = grid_for(t1 - t0, EXPAND_BLOCK, sms * 8);
+      k_expand<<<blocks, EXPAND_BLOCK, 0, st>>>(a);
+      res->launches++;
+      res->chunks++;
+      MG_CK(cudaGetLastError());
+      cur[lvl] = t1;
+      if (writes[lvl]) {
+        MG_CK(cudaMemcpyAsync(&ws->h_ctr[0], ws->ctr + C_OUT, 8, cudaMemcpyDeviceToHost, st));
+        MG_CK(cudaStreamSynchronize(st));
+        const uint64_t rows = ws->h_ctr[0];
+        if (rows > cap) return set_error(MG_E_CUDA, "level table overflow (%llu > %llu)",
+                                         (unsigned long long)rows, (unsigned long long)cap);
+        if (rows > 0) {
+          R[lvl + 1] = uint32_t(rows);
+          ++lvl;
+          need_work = true;
+        }
+      }
+    } else {
+      if (lvl == 0) break;
+      --lvl;
+    }
+  }
+  MG_CK(cudaEventRecord(ws->ev1, st));
+  MG_CK(cudaMemcpyAsync(ws->h_ctr, ws->ctr, C_NUM * 8, cudaMemcpyDeviceToHost, st));
+  MG_CK(cudaMemcpyAsync(counts_out, ws->counts, nq * 8ull, cudaMemcpyDeviceToHost, st));
+  MG_CK(cudaStreamSynchronize(st));
+  MG_CK(cudaGetLastError());
+  float ms = 0;
+  MG_CK(cudaEventElapsedTime(&ms, ws->ev0, ws->ev1));
+  res->ms = ms;
+  res->balg = ws->h_ctr[C_BALG];
+  res->balgc = ws->h_ctr[C_BALGC];
+  res->emitted = ws->h_ctr[C_EMIT];
+  for (int i = 0; i < MAXK + 2 && C_SURV + i < C_NUM; ++i) res->surv[i] = ws->h_ctr[C_SURV + i];
+  if (ws->h_ctr[C_ERR] & ERR_OVERFLOW) return set_error(MG_E_CUDA, "device table overflow");
+  return MG_OK;
+}
+
+// ---- emit: lexicographic sort of rows (LSD over columns) ------------------
+__global__ void k_gather(const uint32_t* __restrict__ src, const uint32_t* __restrict__ perm,
+                         uint32_t* dst, uint64_t n) {
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n;
+       i += uint64_t(gridDim.x) * blockDim.x)
+    dst[i] = src[perm[i]];
+}
+
+__global__ void k_rows_out(uint32_t* const* cols, const uint32_t* __restrict__ perm, uint32_t k,
+                           uint32_t* rows, uint64_t n) {
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n * k;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    uint64_t r = i / k;
+    uint32_t c = uint32_t(i - r * k);
+    rows[i] = cols[c][perm[r]];
+  }
+}
+
+static int sort_and_copy(DevGraph* dg, const EmitBuf& eb, uint32_t k, uint64_t n, uint32_t* h_rows,
+                         uint64_t n_copy) {
+  cudaStream_t st = dg->stream;
+  if (n == 0 || n_copy == 0) return MG_OK;
+  uint32_t *perm_a, *perm_b, *keys_a, *keys_b;
+  MG_CK(cudaMallocAsync((void**)&perm_a, n * 4, st));
+  MG_CK(cudaMallocAsync((void**)&perm_b, n * 4, st));
+  MG_CK(cudaMallocAsync((void**)&keys_a, n * 4, st));
+  MG_CK(cudaMallocAsync((void**)&keys_b, n * 4, st));
+  k_iota<<<grid_for(n, 256, 4096), 256, 0, st>>>(perm_a, uint32_t(n));
+  int end_bit = 1;
+  while (end_bit < 32 && (uint64_t(dg->info.n) > (1ull << end_bit))) ++end_bit;
+  // Global ids may exceed n when the graph uses non-identity ids.
+  end_bit = 32;
+  size_t tmp_bytes = 0;
+  MG_CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys_a, keys_b, perm_a, perm_b,
+                                        int(n), 0, end_bit, st));
+  void* tmp;
+  MG_CK(cudaMallocAsync(&tmp, std::max<size_t>(16, tmp_bytes), st));
+  for (int c = int(k) - 1; c >= 0; --c) {
+    k_gather<<<grid_for(n, 256, 4096), 256, 0, st>>>(eb.col[c], perm_a, keys_a, n);
+    MG_CK(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys_a, keys_b, perm_a, perm_b, int(n),
+                                          0, end_bit, st));
+    std::swap(perm_a, perm_b);
+  }
+  uint32_t** d_cols;
+  MG_CK(cudaMallocAsync((void**)&d_cols, sizeof(uint32_t*) * MAXK, st));
+  MG_CK(cudaMemcpyAsync(d_cols, eb.col, sizeof(uint32_t*) * MAXK, cudaMemcpyHostToDevice, st));
+  uint32_t* d_rows;
+  MG_CK(cudaMallocAsync((void**)&d_rows, n_copy * k * 4, st));
+  k_rows_out<<<grid_for(n_copy * k, 256, 4096), 256, 0, st>>>(d_cols, perm_a, k, d_rows, n_copy);
+  MG_CK(cudaMemcpyAsync(h_rows, d_rows, n_copy * k * 4, cudaMemcpyDeviceToHost, st));
+  MG_CK(cudaStreamSynchronize(st));
+  cudaFreeAsync(perm_a, st);
+  cudaFreeAsync(perm_b, st);
+  cudaFreeAsync(keys_a, st);
+  cudaFreeAsync(keys_b, st);
+  cudaFreeAsync(tmp, st);
+  cudaFreeAsync(d_cols, st);
+  cudaFreeAsync(d_rows, st);
+  MG_CK(cudaStreamSynchronize(st));
+  return MG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Entry-point bodies
+// ---------------------------------------------------------------------------
+struct DeviceGuard {
+  int prev = 0;
+  explicit DeviceGuard(int d) {
+    cudaGetDevice(&prev);
+    cudaSetDevice(d);
+  }
+  ~DeviceGuard() { cudaSetDevice(prev); }
+};
+
+static mg_opts resolve_opts(const mg_opts* o) {
+  mg_opts r;
+  mg_opts_default(&r);
+  if (o) r = *o;
+  return r;
+}
+
+static void fill_stats(mg_stats* st, const PlanDev& P, const RunResult& res, uint64_t count) {
+  if (!st) return;
+  std::memset(st, 0, sizeof(*st));
+  st->k = P.k;
+  for (uint32_t i = 0; i < P.k; ++i) st->order[i] = P.perm[i];
+  for (uint32_t i = 1; i <= P.k && i <= MAXK; ++i) st->level_rows[i] = res.surv[i];
+  st->level_rows[P.k] = count;
+  st->balg_bytes = res.balg;
+  st->balg_count_bytes = res.balgc;
+  st->device_ms = res.ms;
+  st->launches = res.launches;
+  st->chunks = res.chunks;
+}
+
+static int prepare(DevGraph* dg, const mg_csr_view* q, const mg_opts& o, PlanDev* P) {
+  QueryGraph Q;
+  int rc = normalise_query(q, &Q);
+  if (rc) return rc;
+  uint32_t order[MAXK];
+  if ((rc = choose_order(dg, Q, o, order))) return rc;
+  return build_plan(dg, Q, order, P);
+}
+
+int subiso_count(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint64_t* count,
+                 mg_stats* st) {
+  const mg_opts o = resolve_opts(opts);
+  PlanDev P;
+  int rc = prepare(dg, q, o, &P);
+  if (rc) return rc;
+  std::vector<PlanDev> plans(1, P);
+  RunResult res;
+  uint64_t c = 0;
+  if ((rc = run_levels(dg, plans, true, nullptr, o, &c, &res))) return rc;
+  *count = c;
+  fill_stats(st, P, res, c);
+  return MG_OK;
+}
+
+int subiso_emit(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint32_t* rows,
+                uint64_t cap_rows, uint64_t* n_rows, mg_stats* st) {
+  const mg_opts o = resolve_opts(opts);
+  PlanDev P;
+  int rc = prepare(dg, q, o, &P);
+  if (rc) return rc;
+  std::vector<PlanDev> plans(1, P);
+  RunResult res;
+  uint64_t c = 0;
+  if ((rc = run_levels(dg, plans, true, nullptr, o, &c, &res))) return rc;
+  *n_rows = c;
+  if (c >= (1ull << 31))
+    return set_error(MG_E_LIMIT, "%llu matches: emit supports fewer than 2^31 rows",
+                     (unsigned long long)c);
+  EmitBuf eb;
+  eb.cap = c;
+  cudaStream_t s = dg->stream;
+  for (uint32_t j = 0; j < P.k; ++j)
+    MG_CK(cudaMallocAsync((void**)&eb.col[j], std::max<uint64_t>(c, 1) * 4, s));
+  RunResult res2;
+  uint64_t c2 = 0;
+  rc = run_levels(dg, plans, false, &eb, o, &c2, &res2);
+  if (rc == MG_OK && res2.emitted != c)
+    rc = set_error(MG_E_CUDA, "emit pass produced %llu rows, count pass %llu",
+                   (unsigned long long)res2.emitted, (unsigned long long)c);
+  if (rc == MG_OK) rc = sort_and_copy(dg, eb, P.k, c, rows, std::min(c, cap_rows));
+  for (uint32_t j = 0; j < P.k; ++j) cudaFreeAsync(eb.col[j], s);
+  cudaStreamSynchronize(s);
+  if (rc) return rc;
+  res2.balg = res.balg;
+  res2.balgc = res.balgc;
+  fill_stats(st, P, res2, c);
+  if (st) st->device_ms = res.ms + res2.ms;
+  if (c > cap_rows)
+    return set_error(MG_E_CAPACITY, "%llu matches, %llu rows written",
+                     (unsigned long long)c, (unsigned long long)cap_rows);
+  return MG_OK;
+}
+
+int subiso_batch(DevGraph* dg, const mg_csr_view* const* qs, uint32_t nq, const mg_opts* opts,
+                 uint64_t* counts, mg_stats* st) {
+  const mg_opts o = resolve_opts(opts);
+  std::vector<PlanDev> plans(nq);
+  for (uint32_t i = 0; i < nq; ++i) {
+    int rc = prepare(dg, qs[i], o, &plans[i]);
+    if (rc) return set_error(rc, "query %u: %s", i, last_error_cstr());
+  }
+  RunResult res;
+  int rc = run_levels(dg, plans, true, nullptr, o, counts, &res);
+  if (rc) return rc;
+  if (st) {
+    std::memset(st, 0, sizeof(*st));
+    st->balg_bytes = res.balg;
+    st->balg_count_bytes = res.balgc;
+    st->device_ms = res.ms;
+    st->launches = res.launches;
+    st->chunks = res.chunks;
+  }
+  return MG_OK;
+}
+
+}  // namespace mg
+
+// ---------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* mg_last_error(void) { return mg::last_error_cstr(); }
+const char* mg_version(void) { return "mg_subiso 0.1 (sm_100a)"; }
+
+void mg_opts_default(mg_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->order = MG_ORDER_REFERENCE;
+  o->filters = MG_FILTER_ALL;
+}
+
+#define MG_ENTRY(dgraph)                                              \
+  mg::clear_error();                                                  \
+  if (!(dgraph)) return mg::set_error(MG_E_ARG, "null graph handle"); \
+  auto* dg = static_cast<mg::DevGraph*>(dgraph);                      \
+  std::lock_guard<std::mutex> lock(dg->mu);                           \
+  mg::DeviceGuard guard(dg->device)
+
+int mg_plan_order(void* dgraph, const mg_csr_view* q, const mg_opts* opts, uint32_t* order,
+                  uint32_t* k) {
+  mg::clear_error();
+  if (!q || !order || !k) return mg::set_error(MG_E_ARG, "null argument");
+  mg::QueryGraph Q;
+  int rc = mg::normalise_query(q, &Q);
+  if (rc) return rc;
+  const mg_opts o = mg::resolve_opts(opts);
+  if (!dgraph) {
+    if (o.order != MG_ORDER_REFERENCE && o.order != MG_ORDER_GIVEN)
+      return mg::set_error(MG_E_ARG, "this order needs a graph handle");
+    rc = mg::choose_order(nullptr, Q, o, order);
+  } else {
+    auto* dg = static_cast<mg::DevGraph*>(dgraph);
+    std::lock_guard<std::mutex> lock(dg->mu);
+    mg::DeviceGuard guard(dg->device);
+    rc = mg::choose_order(dg, Q, o, order);
+  }
+  if (rc) return rc;
+  *k = Q.k;
+  return MG_OK;
+}
+
+int mg_subiso_count_ex(void* dgraph, const mg_csr_view* q, const mg_opts* opts, uint64_t* count,
+                       mg_stats* st) {
+  MG_ENTRY(dgraph);
+  if (!q || !count) return mg::set_error(MG_E_ARG, "null argument");
+  try {
+    return mg::subiso_count(dg, q, opts, count, st);
+  } catch (const std::bad_alloc&) {
+    return mg::set_error(MG_E_OOM, "host allocation failed");
+  }
+}
+
+int mg_subiso_count(void* dgraph, const mg_csr_view* q, const mg_opts* opts, uint64_t* count) {
+  return mg_subiso_count_ex(dgraph, q, opts, count, nullptr);
+}
+
+int mg_subiso_emit_ex(void* dgraph, const mg_csr_view* q, const mg_opts* opts, uint32_t* rows,
+                      uint64_t cap_rows, uint64_t* n_rows, mg_stats* st) {
+  MG_ENTRY(dgraph);
+  if (!q || !n_rows || (cap_rows && !rows)) return mg::set_error(MG_E_ARG, "null argument");
+  try {
+    return mg::subiso_emit(dg, q, opts, rows, cap_rows, n_rows, st);
+  } catch (const std::bad_alloc&) {
+    return mg::set_error(MG_E_OOM, "host allocation failed");
+  }
+}
+
+int mg_subiso_emit(void* dgraph, const mg_csr_view* q, const mg_opts* opts, uint32_t* rows,
+                   uint64_t cap_rows, uint64_t* n_rows) {
+  return mg_subiso_emit_ex(dgraph, q, opts, rows, cap_rows, n_rows, nullptr);
+}
+
+int mg_subiso_batch_count_ex(void* dgraph, const mg_csr_view* const* qs, uint32_t nq,
+                             const mg_opts* opts, uint64_t* counts, mg_stats* st) {
+  MG_ENTRY(dgraph);
+  if (!qs || !counts || nq == 0) return mg::set_error(MG_E_ARG, "null argument or empty batch");
+  try {
+    return mg::subiso_batch(dg, qs, nq, opts, counts, st);
+  } catch (const std::bad_alloc&) {
+    return mg::set_error(MG_E_OOM, "host allocation failed");
+  }
+}
+
+int mg_subiso_batch_count(void* dgraph, const mg_csr_view* const* qs, uint32_t nq,
+                          const mg_opts* opts, uint64_t* counts) {
+  return mg_subiso_batch_count_ex(dgraph, qs, nq, opts, counts, nullptr);
+}
+
+}  // extern "C"

@@ -1,0 +1,228 @@
+"""Subgraph isomorphism over a device-resident data graph.
+
+Host-side mirror of the reference's subiso entry points:
+
+* ``SubIso(pattern_path, data_graph_path, data_graph_edgelist_path,
+  output_path).Run()`` — core/task/gpu_task/subiso.cuh:43-51, subiso.cu:236-260;
+* ``MatrixGraph(scheduler).Run(TaskType.kSubIso, task)`` —
+  core/matrixgraph.cuh:36-42, core/matrixgraph.cu:30-46.
+
+The reference prints a capped, non-exact join row count and exits the
+process on CUDA errors (core/util/cuda_check.cuh:8-14); here ``Run`` stores
+the exact count (and, in emit mode, the sorted matches), writes them to
+``output_path`` when one is given, and raises :class:`MGError` on failure.
+All device work goes through libmg_subiso.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import os
+import time
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib as L
+from .graph import CSRGraph
+
+ORDERS = {"reference": L.MG_ORDER_REFERENCE, "heuristic": L.MG_ORDER_REFERENCE,
+          "strong": L.MG_ORDER_STRONG, "learned": L.MG_ORDER_LEARNED,
+          "given": L.MG_ORDER_GIVEN}
+
+
+def make_opts(order="reference", filters=L.MG_FILTER_ALL, chunk_rows=0, given_order=None,
+              model=None, root_range=None, mem_budget_bytes=0, persistent=0,
+              block=0, merge_min=0):
+    o = L.default_opts()
+    o.order = ORDERS[order] if isinstance(order, str) else int(order)
+    o.filters = filters
+    o.chunk_rows = chunk_rows
+    o.mem_budget_bytes = mem_budget_bytes
+    o.persistent = persistent
+    o.block = block
+    o.merge_min = merge_min
+    keep = None
+    if given_order is not None:
+        keep = np.ascontiguousarray(np.asarray(given_order, dtype=np.uint32))
+        o.given_order = keep.ctypes.data_as(L.P32)
+        o.order = L.MG_ORDER_GIVEN
+    if model is not None:
+        o.model = model.handle if hasattr(model, "handle") else model
+    if root_range is not None:
+        o.root_begin, o.root_end = int(root_range[0]), int(root_range[1])
+    return o, keep
+
+
+def stats_dict(st: L.Stats) -> dict:
+    k = st.k
+    return {"k": k, "order": list(st.order[:k]), "level_rows": list(st.level_rows[:k + 1]),
+            "balg_bytes": st.balg_bytes, "balg_count_bytes": st.balg_count_bytes,
+            "device_ms": st.device_ms, "launches": st.launches, "chunks": st.chunks}
+
+
+def plan_order(q: CSRGraph, order="reference", graph: "DeviceGraph | None" = None,
+               given_order=None, model=None) -> list[int]:
+    o, keep = make_opts(order=order, given_order=given_order, model=model)
+    out = (C.c_uint32 * L.MG_MAX_QUERY_VERTICES)()
+    k = C.c_uint32()
+    L.check(L.lib.mg_plan_order(graph.handle if graph else None, C.byref(q.view), C.byref(o),
+                                out, C.byref(k)))
+    return list(out[:k.value])
+
+
+class DeviceGraph:
+    """A data graph resident on one GPU with its derived indices."""
+
+    def __init__(self, g: CSRGraph, device: int = 0):
+        h = C.c_void_p()
+        L.check(L.lib.mg_graph_upload(C.byref(g.view), device, C.byref(h)))
+        self.handle = h.value
+        self.device = device
+
+    @property
+    def info(self) -> dict:
+        i = L.GraphInfo()
+        L.check(L.lib.mg_graph_get_info(self.handle, C.byref(i)))
+        return {f: getattr(i, f) for f, _ in L.GraphInfo._fields_}
+
+    def count(self, q: CSRGraph, stats: bool = False, **kw):
+        o, keep = make_opts(**kw)
+        c = C.c_uint64()
+        st = L.Stats()
+        L.check(L.lib.mg_subiso_count_ex(self.handle, C.byref(q.view), C.byref(o), C.byref(c),
+                                         C.byref(st)))
+        return (c.value, stats_dict(st)) if stats else c.value
+
+    def emit(self, q: CSRGraph, cap: int | None = None, stats: bool = False, **kw):
+        """Sorted matches, one row of k global ids per match (query-id order)."""
+        o, keep = make_opts(**kw)
+        if cap is None:
+            cap = self.count(q, **kw)
+        rows = np.zeros((max(cap, 1), q.n), dtype=np.uint32)
+        n = C.c_uint64()
+        st = L.Stats()
+        rc = L.lib.mg_subiso_emit_ex(self.handle, C.byref(q.view), C.byref(o),
+                                     rows.ctypes.data_as(L.P32), cap, C.byref(n), C.byref(st))
+        if rc not in (L.MG_OK, L.MG_E_CAPACITY):
+            L.check(rc)
+        out = rows[:min(cap, n.value)]
+        if stats:
+            return out, n.value, stats_dict(st)
+        return out
+
+    def batch_count(self, qs: Sequence[CSRGraph], stats: bool = False, **kw):
+        o, keep = make_opts(**kw)
+        arr = (C.POINTER(L.CsrView) * len(qs))(*[C.pointer(q.view) for q in qs])
+        counts = np.zeros(len(qs), dtype=np.uint64)
+        st = L.Stats()
+        L.check(L.lib.mg_subiso_batch_count_ex(self.handle, arr, len(qs), C.byref(o),
+                                               counts.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                               C.byref(st)))
+        return (counts, stats_dict(st)) if stats else counts
+
+    def plan_order(self, q: CSRGraph, order="reference", **kw) -> list[int]:
+        return plan_order(q, order=order, graph=self, **kw)
+
+    def free(self) -> None:
+        if self.handle:
+            L.lib.mg_graph_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def shard_roots(n_roots: int, rank: int, world: int) -> tuple[int, int]:
+    """Contiguous level-0 candidate range of one rank (independent shards)."""
+    base, rem = divmod(n_roots, world)
+    begin = rank * base + min(rank, rem)
+    return begin, begin + base + (1 if rank < rem else 0)
+
+
+# ---- reference-shaped task / runtime ------------------------------------------
+class TaskType(enum.IntEnum):
+    """core/common/types.h:47-60."""
+    kGEMM = 0
+    kMatrixAnalysis = 1
+    kPPRQuery = 2
+    kSubIso = 3
+    kGARMatch = 4
+    kCPUSubIso = 5
+    kWCC = 6
+    kSSSP = 7
+    kBFS = 8
+    kPageRank = 9
+    kGEMV = 10
+
+
+class SchedulerType(enum.IntEnum):
+    """core/components/scheduler/scheduler.h (ignored by subiso, as in the reference)."""
+    kCHBL = 0
+    kEvenSplit = 1
+    kRoundRobin = 2
+
+
+class SubIso:
+    """``SubIso`` task: pattern and data graph CSR directories in, exact matches out."""
+
+    def __init__(self, pattern_path: str, data_graph_path: str,
+                 data_graph_edgelist_path: str = "", output_path: str = "",
+                 mode: str = "count", order: str = "reference", device: int = 0,
+                 model=None):
+        self.pattern_path = pattern_path
+        self.data_graph_path = data_graph_path
+        self.data_graph_edgelist_path = data_graph_edgelist_path  # unused, as in the reference
+        self.output_path = output_path
+        self.mode = mode
+        self.order = order
+        self.device = device
+        self.model = model
+        self.count = None
+        self.rows = None
+        self.timings = {}
+
+    def LoadData(self):
+        self.p_ = CSRGraph.Read(self.pattern_path)
+        self.g_ = CSRGraph.Read(self.data_graph_path)
+
+    def Run(self):
+        t0 = time.perf_counter()
+        self.LoadData()
+        t1 = time.perf_counter()
+        dg = DeviceGraph(self.g_, self.device)
+        try:
+            t2 = time.perf_counter()
+            self.count = dg.count(self.p_, order=self.order, model=self.model)
+            if self.mode == "emit":
+                self.rows = dg.emit(self.p_, cap=self.count, order=self.order, model=self.model)
+            t3 = time.perf_counter()
+        finally:
+            dg.free()
+        self.timings = {"load_s": t1 - t0, "upload_s": t2 - t1, "match_s": t3 - t2}
+        if self.output_path:
+            self.Write(self.output_path)
+        return self.count
+
+    def Write(self, path: str):
+        os.makedirs(os.path.dirname(os.path.abspath(path)) or ".", exist_ok=True)
+        with open(path, "w") as f:
+            f.write(f"{self.count}\n")
+            if self.rows is not None:
+                for r in self.rows:
+                    f.write(",".join(str(int(x)) for x in r) + "\n")
+
+
+class MatrixGraph:
+    """Runtime dispatch (core/matrixgraph.cu:30-79): only kSubIso is served."""
+
+    def __init__(self, scheduler: SchedulerType = SchedulerType.kCHBL):
+        self.scheduler = scheduler
+
+    def Run(self, task_type: TaskType, task):
+        if task_type != TaskType.kSubIso:
+            raise L.MGError(L.MG_E_ARG, f"task type {TaskType(task_type).name} is not served")
+        return task.Run()

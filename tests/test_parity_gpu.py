@@ -1,0 +1,191 @@
+"""GPU parity: the CUDA path (through the C-ABI) against the oracle and brute force."""
+import itertools
+import os
+
+import numpy as np
+import pytest
+
+import matrixgraph_b200 as mg
+import oracle as O
+from matrixgraph_b200 import _lib as L
+from helpers import (brute_count, brute_rows, complete, graph, oracle_count, oracle_rows,
+                     random_graph, random_query, undirected)
+from test_oracle import GOLDEN, QUERIES, golden_cases, golden_graph, golden_query
+
+pytestmark = pytest.mark.gpu
+
+C4 = [(0, 1), (1, 2), (2, 3), (3, 0)]
+
+
+@pytest.fixture(scope="module")
+def c1():
+    """Chung-Lu n=10,000, beta 2.5, mean degree 10, 8 uniform labels; 4-cycle query."""
+    g = mg.chung_lu()
+    q = mg.CSRGraph.query(4, C4, mg.gen_labels(4, 8, "uniform", seed=2))
+    dg = mg.DeviceGraph(g)
+    yield g, q, dg
+    dg.free()
+
+
+def test_c1_count_rows_and_stats(c1):
+    g, q, dg = c1
+    want = oracle_count(g, q, threads=4)
+    got, st = dg.count(q, stats=True)
+    assert got == want["count"] > 0
+    assert st["level_rows"] == want["level_rows"]
+    assert st["balg_bytes"] == want["balg"]
+    assert st["balg_count_bytes"] == want["balg_count"]
+    rows = dg.emit(q)
+    assert np.array_equal(rows, oracle_rows(g, q))
+
+
+def test_c1_all_orders_and_chunks(c1):
+    g, q, dg = c1
+    want = oracle_count(g, q)["count"]
+    for perm in itertools.permutations(range(4)):
+        for chunk in (0, 97):
+            r = oracle_count(g, q, order=perm)
+            c, st = dg.count(q, given_order=perm, chunk_rows=chunk, stats=True)
+            assert c == want
+            assert st["level_rows"] == r["level_rows"]
+            assert st["balg_bytes"] == r["balg"]
+    for f in (0, 1, 2):
+        assert dg.count(q, filters=f) == want
+
+
+def test_graph_info(c1):
+    g, q, dg = c1
+    info = dg.info
+    assert info["n"] == 10000 and info["n_labels"] == 8 and info["symmetric"] == 1
+    assert info["m_out"] == g.m_out
+
+
+@pytest.mark.parametrize("seed", range(16))
+def test_random_undirected(seed):
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(8, 40))
+    edges, labels = random_graph(rng, n, 0.3, int(rng.integers(1, 4)))
+    g = graph(n, edges, labels)
+    dg = mg.DeviceGraph(g)
+    for _ in range(4):
+        k = int(rng.integers(1, 7))
+        qe, ql = random_query(rng, k, 0.35, max(labels) + 1)
+        q = mg.CSRGraph.query(k, qe, ql)
+        want = oracle_count(g, q)
+        c, st = dg.count(q, stats=True, chunk_rows=int(rng.choice([0, 1, 5, 64])))
+        assert c == want["count"]
+        assert st["level_rows"] == want["level_rows"]
+        if n <= 14 and k <= 5:
+            assert c == brute_count(n, undirected(edges), labels, k, undirected(qe), ql)
+        rows = dg.emit(q)
+        assert np.array_equal(rows, oracle_rows(g, q))
+    dg.free()
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_random_directed_self_loops(seed):
+    rng = np.random.default_rng(500 + seed)
+    n = int(rng.integers(6, 24))
+    edges, labels = random_graph(rng, n, 0.3, 2, directed=True, self_loops=True)
+    g = graph(n, edges, labels, symmetric=False)
+    dg = mg.DeviceGraph(g)
+    assert dg.info["symmetric"] == 0
+    for t in range(4):
+        k = int(rng.integers(1, 5))
+        qe, ql = random_query(rng, k, 0.3, 2, directed=True)
+        if t % 2:
+            qe = qe + [(k - 1, k - 1)]
+        q = mg.CSRGraph.query(k, qe, ql, directed=True)
+        want = oracle_count(g, q)
+        c, st = dg.count(q, stats=True)
+        assert c == want["count"]
+        assert st["balg_bytes"] == want["balg"]
+        if n <= 12:
+            assert c == brute_count(n, edges, labels, k, qe, ql)
+        assert np.array_equal(dg.emit(q), oracle_rows(g, q))
+    dg.free()
+
+
+def test_golden_counts_gpu():
+    cache = {}
+    for name, lname, key, want in golden_cases():
+        if (name, lname) not in cache:
+            cache[(name, lname)] = (golden_graph(name, lname), None)
+            cache[(name, lname)] = (cache[(name, lname)][0],
+                                    mg.DeviceGraph(cache[(name, lname)][0]))
+        g, dg = cache[(name, lname)]
+        assert dg.count(golden_query(key)) == want, (name, lname, key)
+    for g, dg in cache.values():
+        dg.free()
+
+
+def test_edge_cases():
+    g = complete(6, [0, 0, 0, 1, 1, 1])
+    dg = mg.DeviceGraph(g)
+    # absent label, single vertex, query larger than the graph, disconnected query
+    assert dg.count(mg.CSRGraph.query(3, [(0, 1), (1, 2)], [0, 7, 0])) == 0
+    assert dg.count(mg.CSRGraph.query(1, [], [1])) == 3
+    assert dg.count(mg.CSRGraph.query(7, [(i, i + 1) for i in range(6)], [0] * 7)) == 0
+    qd = mg.CSRGraph.query(4, [(0, 1), (2, 3)], [0, 0, 1, 1])
+    assert dg.count(qd) == oracle_count(g, qd)["count"] == 6 * 6
+    assert np.array_equal(dg.emit(qd), oracle_rows(g, qd))
+    assert dg.emit(mg.CSRGraph.query(3, [(0, 1), (1, 2)], [0, 7, 0])).shape == (0, 3)
+    dg.free()
+
+
+def test_emit_capacity():
+    g = complete(7)
+    dg = mg.DeviceGraph(g)
+    q = mg.CSRGraph.query(3, [(0, 1), (1, 2), (2, 0)], [0, 0, 0])
+    full = dg.emit(q)
+    assert full.shape == (210, 3)
+    part, n, _ = dg.emit(q, cap=50, stats=True)
+    assert n == 210 and np.array_equal(part, full[:50])
+    dg.free()
+
+
+def test_batch_equals_single(c1):
+    g, q, dg = c1
+    qs = [mg.query_random(g, 3 + i % 6, 0.3, seed=1000 + i) for i in range(64)]
+    single = [dg.count(x) for x in qs]
+    assert dg.batch_count(qs).tolist() == single
+    assert dg.batch_count(qs, chunk_rows=333).tolist() == single
+    for x, c in list(zip(qs, single))[:12]:
+        assert oracle_count(g, x)["count"] == c
+
+
+def test_root_ranges_sum(c1):
+    g, q, dg = c1
+    full = dg.count(q)
+    nb = O.bucket_size(O.Graph.from_csr(g), O.query_from_csr(q), mg.plan_order(q))
+    parts = [mg.shard_roots(nb, r, 3) for r in range(3)]
+    got = [dg.count(q, root_range=p) for p in parts]
+    assert sum(got) == full
+    assert got[1] == oracle_count(g, q, root_range=parts[1])["count"]
+
+
+def test_subiso_task_and_runtime(tmp_path, c1):
+    g, q, dg = c1
+    g.Write(str(tmp_path / "g") + "/")
+    q.Write(str(tmp_path / "p") + "/")
+    task = mg.SubIso(str(tmp_path / "p") + "/", str(tmp_path / "g") + "/", "",
+                     str(tmp_path / "out.txt"), mode="emit")
+    mg.MatrixGraph().Run(mg.TaskType.kSubIso, task)
+    assert task.count == dg.count(q)
+    lines = open(tmp_path / "out.txt").read().split()
+    assert int(lines[0]) == task.count and len(lines) == task.count + 1
+
+
+def test_rmat_small_full_parity():
+    g = mg.rmat(14, n_labels=8, label_kind="zipf")
+    dg = mg.DeviceGraph(g)
+    og = O.Graph.from_csr(g)
+    for i, shape in enumerate(mg.SHAPES):
+        q = mg.query_walk(g, shape, seed=2 + i)
+        want = O.count(og, O.query_from_csr(q), threads=8)
+        c, st = dg.count(q, stats=True)
+        assert c == want["count"], shape
+        assert st["level_rows"] == want["level_rows"], shape
+        assert st["balg_count_bytes"] == want["balg_count"], shape
+        assert dg.count(q, order="strong") == c
+    dg.free()
