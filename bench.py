@@ -44,14 +44,18 @@ def parse():
                    help="target CPU time of the oracle baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--queries", default="",
+                   help="comma-separated subset of the query shapes (profiling runs)")
     return p.parse_args()
 
 
-def workload(scale):
+def workload(scale, only=""):
     import matrixgraph_b200 as mg
     g = mg.rmat(scale, 16, 0.57, 0.19, 0.19, seed=0, n_labels=32, label_kind="zipf",
                 zipf_s=1.0, label_seed=1)
-    qs = [mg.query_walk(g, s, seed=SHAPE_SEEDS + i) for i, s in enumerate(mg.SHAPES)]
+    keep = [x for x in only.split(",") if x]
+    qs = [mg.query_walk(g, s, seed=SHAPE_SEEDS + i) for i, s in enumerate(mg.SHAPES)
+          if not keep or s in keep]
     return g, qs
 
 
@@ -191,7 +195,7 @@ def run_reference(args):
     world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
     if rank != 0:
         return
-    g, qs = workload(args.scale)
+    g, qs = workload(args.scale, args.queries)
     import oracle as O
     threads = os.cpu_count() or 1
     og = O.Graph.from_csr(g)
@@ -244,7 +248,7 @@ def run_mine(args):
     device = local
     torch.cuda.set_device(device)
     t0 = time.perf_counter()
-    g, qs = workload(args.scale)
+    g, qs = workload(args.scale, args.queries)
     gen_s = time.perf_counter() - t0
     buckets = first_bucket_sizes(g, qs)
     ranges = [mg.shard_roots(nb, rank, world) if world > 1 else None for nb in buckets]
@@ -312,7 +316,7 @@ def run_mine(args):
             dg2.count(q, root_range=rr)
         dg2.free()
         e2e_times.append(time.perf_counter() - t0)
-    e2e_s = statistics.median(e2e_times)
+    e2e_s = statistics.median(e2e_times) if e2e_times else float("nan")
     if world > 1:
         t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{device}")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -336,9 +340,9 @@ def run_mine(args):
                 "config": config(args.scale, g), "queries_per_s": len(qs) / (ms_step / 1e3),
                 "counts": counts, "host_ms_per_step": host_ms,
                 "roofline": roofline, "cpu_baseline": cpu,
-                "e2e": {"value": emb / e2e_s, "unit": "embeddings/s",
-                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                        "seconds_per_step": e2e_s},
+                "e2e": ({"value": emb / e2e_s, "unit": "embeddings/s",
+                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                         "seconds_per_step": e2e_s} if e2e_times else None),
                 "clocks": clocks, "gpu_launches": launches * args.steps,
                 "graph": {"n": info["n"], "m_out": info["m_out"],
                           "device_bytes": info["device_bytes"], "max_degree": info["max_degree"],

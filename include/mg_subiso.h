@@ -101,6 +101,10 @@ typedef struct mg_opts {
   uint64_t mem_budget_bytes; /* cap on enumeration scratch; 0 = auto        */
   uint64_t root_begin;       /* level-0 candidates [root_begin, root_end) of  */
   uint64_t root_end;         /* the first position's label bucket; 0,0 = all  */
+  uint32_t no_tail;          /* closed-form count of a two-position pendant
+                                tail (count mode): 0 = when it pays off,
+                                1 = never, 2 = always                        */
+  uint32_t _reserved;
 } mg_opts;
 
 /* Per-call statistics (optional out-parameter of the *_ex entry points). */

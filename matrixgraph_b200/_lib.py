@@ -60,7 +60,8 @@ class Opts(C.Structure):
                 ("model", C.c_void_p), ("chunk_rows", C.c_uint64), ("block", C.c_uint32),
                 ("merge_min", C.c_uint32), ("spin_limit", C.c_uint32),
                 ("persistent", C.c_uint32), ("mem_budget_bytes", C.c_uint64),
-                ("root_begin", C.c_uint64), ("root_end", C.c_uint64)]
+                ("root_begin", C.c_uint64), ("root_end", C.c_uint64),
+                ("no_tail", C.c_uint32), ("_reserved", C.c_uint32)]
 
 
 class Stats(C.Structure):

@@ -58,6 +58,16 @@ struct PlanDev {
   uint32_t samelab[MAXK];              // positions j < i with the same label
   uint32_t guar[MAXK];                 // last position: m(j) surely in slice
   uint32_t perm[MAXK];
+  // Two-position pendant tail (count mode): position a = k-2 has the single
+  // backward neighbour tail_p (direction tail_da), position b = k-1 has the
+  // single backward neighbour a (direction tail_db), neither has a self-loop,
+  // and every earlier position labelled like b is tail_p itself with
+  // matching directions.  Rows of prefix length k-2 are then counted in
+  // closed form from a per-vertex two-hop aggregate.
+  uint32_t tail2;
+  uint32_t tail_p, tail_da, tail_db;
+  uint32_t tail_Ia;  // positions i < a labelled like position a
+  uint32_t tail_J;   // positions j < a labelled like position b
 };
 
 struct Workspace;  // enumeration scratch (mg_enum.cu)

@@ -51,6 +51,9 @@ struct Workspace {
   uint8_t* dci[MAXK] = {};
   uint64_t* bsum = nullptr;
   uint32_t bsum_cap = 0;
+  uint32_t* tile_row = nullptr;  // first row of every expand tile of a segment
+  unsigned long long* tailA = nullptr;   // per-vertex two-hop aggregates (n each)
+  unsigned long long* tailAD = nullptr;
   unsigned long long* ctr = nullptr;     // device counters
   unsigned long long* h_ctr = nullptr;   // pinned mirror
   unsigned long long* counts = nullptr;  // per query
@@ -63,7 +66,10 @@ struct Workspace {
 };
 
 // Counter slots.
-enum : int { C_OUT = 0, C_BALG = 1, C_BALGC = 2, C_ERR = 3, C_EMIT = 4, C_SURV = 8, C_NUM = 8 + MAXK + 2 };
+enum : int {
+  C_OUT = 0, C_BALG = 1, C_BALGC = 2, C_ERR = 3, C_EMIT = 4, C_PROBE_BALG = 5,
+  C_PROBE_BALGC = 6, C_SURV = 8, C_NUM = 8 + MAXK + 2
+};
 
 void free_workspace(Workspace* ws) {
   if (!ws) return;
@@ -90,6 +96,8 @@ static int ws_alloc(Workspace* ws, void** p, size_t bytes) {
 
 constexpr uint64_t kDefaultCap = 1ull << 24;
 constexpr int SCAN_TILE = 4096;
+constexpr int EXPAND_BLOCK = 256;                 // elements per expand tile
+constexpr uint64_t kSegment = 1ull << 26;         // elements per expand launch
 
 static uint64_t level_row_bytes(int l) { return uint64_t(l) * 4 + 4 + 4 + 8 + 4 + 1; }
 
@@ -112,6 +120,7 @@ static int ensure_ws(DevGraph* dg, uint64_t cap, int levels, uint32_t nq) {
     MG_CK(cudaEventCreate(&ws->ev1));
     ws->bsum_cap = uint32_t((std::max<uint64_t>(cap, ws->rows0) + SCAN_TILE - 1) / SCAN_TILE + 1);
     if ((rc = ws_alloc(ws, (void**)&ws->bsum, uint64_t(ws->bsum_cap) * 8))) return rc;
+    if ((rc = ws_alloc(ws, (void**)&ws->tile_row, (kSegment / EXPAND_BLOCK + 2) * 4))) return rc;
   }
   if (ws->counts_cap < nq) {
     int rc;
@@ -164,6 +173,10 @@ struct StepArgs {
   uint32_t* emit_col[MAXK];
   uint64_t emit_cap;
   uint64_t root_begin, root_end;  // level-0 candidate range (root_end 0: all)
+  const uint32_t* tile_row;        // first row of each tile of [t0, t1)
+  const unsigned long long* tailA;  // non-null: count tail rows in closed form
+  const unsigned long long* tailAD;
+  uint32_t probe;                   // charge algorithmic bytes to the probe slots
 };
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -230,8 +243,51 @@ __device__ __forceinline__ uint32_t find_row(const uint64_t* __restrict__ woff, 
 // Work kernel: per row, the driving slice (shortest backward slice, or the
 // label bucket for a position without backward neighbours) and the
 // algorithmic-byte charge of extending the row.
+// Closed-form count of one row of prefix length a = k-2 under a two-position
+// pendant tail (PlanDev::tail2).  With I the matched prefix, S = the
+// label-l_a slice of m_p, D(x) = |N_{l_b}(x)| and c(x) = D(x) - [x has a
+// self-loop and l_a == l_b], and A(y) = sum_{x in S(y)} c(x):
+//   count = A(m_p) - sum_{i in Ia, m_i in S} (c(m_i) - #{j in J : m_j in N_{l_b}(m_i)})
+//           - sum_{j in J} |S|                   (every j in J is p itself)
+// Also returns the number of length-(k-1) prefixes |S \ I| and their
+// algorithmic bytes sum_{x in S \ I} D(x).
+__device__ __forceinline__ void tail_count(const StepArgs& a, const PlanDev& P, uint64_t r,
+                                           unsigned long long& cnt, unsigned long long& pre,
+                                           unsigned long long& dsum) {
+  const GraphDev& g = a.g;
+  const uint32_t ia = P.k - 2;
+  const uint32_t la = P.label[ia], lb = P.label[ia + 1];
+  const uint32_t da = P.tail_da, db = P.tail_db;
+  const uint32_t mp = a.in.col[P.tail_p][r];
+  uint32_t s, e;
+  slice_of(g, da, mp, la, s, e);
+  long long c = (long long)a.tailA[mp];
+  long long d = (long long)a.tailAD[mp];
+  unsigned long long inS = 0;
+  for (uint32_t mi = P.tail_Ia; mi; mi &= mi - 1) {
+    const uint32_t i2 = __ffs(mi) - 1;
+    const uint32_t x = a.in.col[i2][r];
+    if (!contains(g.adj[da], s, e, x)) continue;
+    inS += 1;
+    uint32_t xs, xe;
+    slice_of(g, db, x, lb, xs, xe);
+    long long cx = (long long)(xe - xs);
+    d -= cx;
+    if (la == lb && has_self(g, x)) cx -= 1;
+    for (uint32_t mj = P.tail_J; mj; mj &= mj - 1) {
+      const uint32_t j = __ffs(mj) - 1;
+      if (contains(g.adj[db], xs, xe, a.in.col[j][r])) cx -= 1;
+    }
+    c -= cx;
+  }
+  c -= (long long)__popc(P.tail_J) * (long long)(e - s);
+  cnt = (unsigned long long)c;
+  pre = (unsigned long long)(e - s) - inS;
+  dsum = (unsigned long long)d;
+}
+
 __global__ void __launch_bounds__(256) k_work(StepArgs a) {
-  unsigned long long bal = 0, balc = 0;
+  unsigned long long bal = 0, balc = 0, tcnt = 0, tpre = 0;
   const uint32_t i = a.level;
   const GraphDev& g = a.g;
   for (uint64_t r = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; r < a.R;
@@ -243,6 +299,24 @@ __global__ void __launch_bounds__(256) k_work(StepArgs a) {
     uint32_t best, bs = 0;
     uint8_t bci = DCI_BUCKET;
     unsigned long long ch = 0, chc = 0;
+    if (a.tailA && P.tail2 && i + 2 == P.k) {
+      // position a = k-2: one backward slice; position b counted in closed form
+      const uint32_t cs = P.cons[i][0];
+      uint32_t s, e;
+      slice_of(g, cs >> 8, a.in.col[cs & 0xFF][r], lab, s, e);
+      unsigned long long cnt, pre, dsum;
+      tail_count(a, P, r, cnt, pre, dsum);
+      ch = 8ull + 4ull * (e - s) + 8ull * pre + 4ull * dsum;
+      chc = 8ull + 4ull * (e - s) + 8ull * pre;
+      tcnt += cnt;
+      tpre += pre;
+      a.work[r] = 0;
+      a.dstart[r] = 0;
+      a.dci[r] = 0;
+      bal += ch;
+      balc += chc;
+      continue;
+    }
     if (P.zero) {
       best = 0;
     } else if (nc == 0) {
@@ -280,8 +354,49 @@ __global__ void __launch_bounds__(256) k_work(StepArgs a) {
   bal = warp_sum(bal);
   balc = warp_sum(balc);
   if ((threadIdx.x & 31) == 0 && (bal | balc)) {
-    atomicAdd(&a.ctr[C_BALG], bal);
-    atomicAdd(&a.ctr[C_BALGC], balc);
+    atomicAdd(&a.ctr[a.probe ? C_PROBE_BALG : C_BALG], bal);
+    atomicAdd(&a.ctr[a.probe ? C_PROBE_BALGC : C_BALGC], balc);
+  }
+  if (a.tailA) {  // single-query mode only
+    tcnt = warp_sum(tcnt);
+    tpre = warp_sum(tpre);
+    if ((threadIdx.x & 31) == 0) {
+      if (tcnt) atomicAdd(&a.counts[0], tcnt);
+      if (a.stats && tpre) atomicAdd(&a.ctr[C_SURV + i + 1], tpre);
+      if (a.stats && tcnt) atomicAdd(&a.ctr[C_SURV + i + 2], tcnt);
+    }
+  }
+}
+
+// Two-hop aggregates over the label bucket of position p's label:
+// A(y) = sum_{x in N^{da}_{la}(y)} (|N^{db}_{lb}(x)| - [x self-loop, la == lb]),
+// AD(y) = sum_{x in N^{da}_{la}(y)} |N^{db}_{lb}(x)|.  Warp per vertex.
+__global__ void __launch_bounds__(256) k_tail_aggregate(GraphDev g, uint32_t bucket_lab,
+                                                        uint32_t da, uint32_t la, uint32_t db,
+                                                        uint32_t lb, unsigned long long* A,
+                                                        unsigned long long* AD) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5;
+  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  const uint32_t b0 = g.bucket_off[bucket_lab], b1 = g.bucket_off[bucket_lab + 1];
+  for (uint64_t w = warp; w < b1 - b0; w += nwarps) {
+    const uint32_t y = g.bucket_vid[b0 + w];
+    uint32_t s, e;
+    slice_of(g, da, y, la, s, e);
+    unsigned long long sa = 0, sd = 0;
+    for (uint32_t j = s + lane; j < e; j += 32) {
+      const uint32_t x = __ldg(g.adj[da] + j);
+      uint32_t xs, xe;
+      slice_of(g, db, x, lb, xs, xe);
+      sd += xe - xs;
+      sa += xe - xs - ((la == lb && has_self(g, x)) ? 1u : 0u);
+    }
+    sa = warp_sum(sa);
+    sd = warp_sum(sd);
+    if (lane == 0) {
+      A[y] = sa;
+      AD[y] = sd;
+    }
   }
 }
 
@@ -374,11 +489,21 @@ __global__ void __launch_bounds__(256) k_scan_apply(const uint32_t* __restrict__
   }
 }
 
-// Expand kernel: one element (row, driving entry) per thread.
-constexpr int EXPAND_BLOCK = 256;
+// First row of every tile of the element range [t0, t1): tile_row[j] is the
+// row holding element t0 + j*EXPAND_BLOCK (clamped to t1 - 1), j = 0..ntiles.
+__global__ void __launch_bounds__(256) k_tile_rows(const uint64_t* __restrict__ woff, uint32_t R,
+                                                   uint64_t t0, uint64_t t1, uint32_t ntiles,
+                                                   uint32_t* tile_row) {
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j <= ntiles;
+       j += gridDim.x * blockDim.x) {
+    uint64_t t = t0 + uint64_t(j) * EXPAND_BLOCK;
+    if (t > t1 - 1) t = t1 - 1;
+    tile_row[j] = find_row(woff, 0, R - 1, t);
+  }
+}
 
+// Expand kernel: one element (row, driving entry) per thread.
 __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
-  __shared__ uint32_t s_rlo, s_rhi;
   const uint32_t i = a.level;
   const GraphDev& g = a.g;
   const uint32_t lane = threadIdx.x & 31;
@@ -389,11 +514,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
   for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const uint64_t tb = a.t0 + tile * EXPAND_BLOCK;
     const uint64_t te = min(tb + EXPAND_BLOCK, a.t1);
-    if (threadIdx.x == 0) s_rlo = find_row(a.woff, 0, a.R - 1, tb);
-    if (threadIdx.x == 32) s_rhi = find_row(a.woff, 0, a.R - 1, te - 1);
-    __syncthreads();
-    const uint32_t rlo = s_rlo, rhi = s_rhi;
-    __syncthreads();
+    const uint32_t rlo = __ldg(a.tile_row + tile), rhi = __ldg(a.tile_row + tile + 1);
     const uint64_t t = tb + threadIdx.x;
     const bool valid = t < te;
     bool ok = false, fin = false, fused = false;
@@ -432,7 +553,11 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
       if (ok && ((P.selfloop_mask >> i) & 1u)) ok = has_self(g, x);
       fin = (i + 1 == P.k);
       fused = !fin && a.count_mode && (i + 2 == P.k) && P.last_o1;
-      if (ok && !fin && a.filters) ok = pass_filters(g, P, i, x, a.filters);
+      // Filters prune positions whose survivors are extended further; the
+      // position before a last position counted in closed form is not
+      // filtered (the closed form already yields 0 for hopeless candidates).
+      if (ok && !fin && a.filters && !(i + 2 == P.k && P.last_o1))
+        ok = pass_filters(g, P, i, x, a.filters);
       if (ok) {
         surv1 += 1;
         if (fin) {
@@ -587,6 +712,28 @@ int build_plan(const DevGraph* dg, const QueryGraph& Q, const uint32_t* order, P
   }
   const uint32_t kl = k - 1;
   P->last_o1 = (k >= 2 && P->ncons[kl] == 1 && !((P->selfloop_mask >> kl) & 1u)) ? 1u : 0u;
+  if (P->last_o1 && k >= 3 && !P->zero) {
+    const uint32_t ia = k - 2;
+    const uint32_t cb = P->cons[kl][0], ca = P->cons[ia][0];
+    if ((cb & 0xFF) == ia && P->ncons[ia] == 1 && !((P->selfloop_mask >> ia) & 1u)) {
+      const uint32_t p = ca & 0xFF, da = ca >> 8, db = cb >> 8;
+      uint32_t Ia = 0, J = 0;
+      for (uint32_t j = 0; j < ia; ++j) {
+        if (P->label[j] == P->label[ia]) Ia |= 1u << j;
+        if (P->label[j] == P->label[kl]) J |= 1u << j;
+      }
+      // every j in J must be p with x in N^{rev db}(m_p) <=> x in N^{da}(m_p)
+      const bool ok = J == 0 || (J == (1u << p) && (sym || da != db));
+      if (ok) {
+        P->tail2 = 1;
+        P->tail_p = p;
+        P->tail_da = da;
+        P->tail_db = db;
+        P->tail_Ia = Ia;
+        P->tail_J = J;
+      }
+    }
+  }
   if (P->last_o1) {
     const uint32_t cs = P->cons[kl][0];
     const uint32_t ws = order[cs & 0xFF], dir = cs >> 8;
@@ -657,7 +804,12 @@ static int run_levels(DevGraph* dg, const std::vector<PlanDev>& plans, bool coun
   const uint32_t nq = uint32_t(plans.size());
   uint32_t kmax = 1;
   for (auto& p : plans) kmax = std::max(kmax, p.k);
-  uint64_t cap = o.chunk_rows ? o.chunk_rows : kDefaultCap;
+  // Default rows per level chunk: scaled with the graph so small graphs do
+  // not reserve gigabytes of scratch; chunking keeps larger results exact.
+  uint64_t auto_cap = 1ull << 16;
+  while (auto_cap < kDefaultCap && auto_cap < 4 * (uint64_t(dg->g.n) + dg->info.m_out))
+    auto_cap <<= 1;
+  uint64_t cap = o.chunk_rows ? o.chunk_rows : auto_cap;
   cap = std::max<uint64_t>(cap, 1);
   if (cap > (1ull << 31)) return set_error(MG_E_ARG, "chunk_rows above 2^31");
   if (o.mem_budget_bytes) {
@@ -713,6 +865,36 @@ static int run_levels(DevGraph* dg, const std::vector<PlanDev>& plans, bool coun
   int lvl = 0;
   bool need_work = true;
   const unsigned sms = 148;
+
+  // Closed-form two-position tail (single query, count mode): enabled once
+  // the elements met at position k-2 outweigh the one-off aggregate pass.
+  const bool tail_possible = count_mode && nq == 1 && plans[0].tail2 && o.no_tail != 1;
+  const bool tail_forced = o.no_tail == 2;
+  const int tail_lvl = int(plans[0].k) - 2;
+  bool tail_ready = false;
+  uint64_t tail_T = 0, tail_cost = 0, extra_balg = 0, extra_balgc = 0;
+  if (tail_possible) {
+    if ((rc = ensure_full_stats(dg))) return rc;
+    const PlanDev& P = plans[0];
+    const uint32_t lp = P.label[P.tail_p], la = P.label[tail_lvl], L = dg->g.L;
+    tail_cost = P.tail_da == 0 ? dg->stats.label_pair_edges[uint64_t(lp) * L + la]
+                               : dg->stats.label_pair_edges[uint64_t(la) * L + lp];
+  }
+  auto launch_work_scan = [&](int l, bool probe) -> int {
+    a.probe = probe ? 1u : 0u;
+    k_work<<<grid_for(R[l], 256, sms * 16), 256, 0, st>>>(a);
+    const uint32_t nb = (R[l] + SCAN_TILE - 1) / SCAN_TILE;
+    k_scan_reduce<<<nb, 256, 0, st>>>(ws->work[l], R[l], ws->bsum);
+    k_scan_bsum<<<1, 1024, 0, st>>>(ws->bsum, nb, ws->woff[l] + R[l]);
+    k_scan_apply<<<nb, 256, 0, st>>>(ws->work[l], R[l], ws->bsum, ws->woff[l]);
+    res->launches += 4;
+    MG_CK(cudaMemcpyAsync(&ws->h_ctr[0], ws->woff[l] + R[l], 8, cudaMemcpyDeviceToHost, st));
+    if (probe)
+      MG_CK(cudaMemcpyAsync(&ws->h_ctr[C_PROBE_BALG], ws->ctr + C_PROBE_BALG, 16,
+                            cudaMemcpyDeviceToHost, st));
+    MG_CK(cudaStreamSynchronize(st));
+    return MG_OK;
+  };
   auto tab = [&](int l) {
     TabPtrs t{};
     for (int j = 0; j < l; ++j) t.col[j] = ws->col[l][j];
@@ -728,21 +910,54 @@ static int run_levels(DevGraph* dg, const std::vector<PlanDev>& plans, bool coun
       a.woff = ws->woff[lvl];
       a.dstart = ws->dstart[lvl];
       a.dci = ws->dci[lvl];
-      k_work<<<grid_for(R[lvl], 256, sms * 16), 256, 0, st>>>(a);
-      const uint32_t nb = (R[lvl] + SCAN_TILE - 1) / SCAN_TILE;
-      k_scan_reduce<<<nb, 256, 0, st>>>(ws->work[lvl], R[lvl], ws->bsum);
-      k_scan_bsum<<<1, 1024, 0, st>>>(ws->bsum, nb, ws->woff[lvl] + R[lvl]);
-      k_scan_apply<<<nb, 256, 0, st>>>(ws->work[lvl], R[lvl], ws->bsum, ws->woff[lvl]);
-      res->launches += 4;
-      MG_CK(cudaMemcpyAsync(&ws->h_ctr[0], ws->woff[lvl] + R[lvl], 8, cudaMemcpyDeviceToHost, st));
-      MG_CK(cudaStreamSynchronize(st));
-      T[lvl] = ws->h_ctr[0];
+      a.tailA = nullptr;
+      a.tailAD = nullptr;
+      const bool at_tail = tail_possible && lvl == tail_lvl;
+      if (at_tail && !tail_ready) {
+        // Probe: plain work pass whose byte charges are kept aside.
+        MG_CK(cudaMemsetAsync(ws->ctr + C_PROBE_BALG, 0, 16, st));
+        if ((rc = launch_work_scan(lvl, true))) return rc;
+        tail_T += ws->h_ctr[0];
+        if (tail_forced || 2 * tail_T >= tail_cost) {
+          if (!ws->tailA) {
+            if ((rc = ws_alloc(ws, (void**)&ws->tailA, uint64_t(dg->g.n) * 8))) return rc;
+            if ((rc = ws_alloc(ws, (void**)&ws->tailAD, uint64_t(dg->g.n) * 8))) return rc;
+          }
+          const PlanDev& P = plans[0];
+          const uint32_t lp = P.label[P.tail_p];
+          const uint64_t nbk = dg->h_bucket_off[lp + 1] - dg->h_bucket_off[lp];
+          k_tail_aggregate<<<grid_for(nbk * 32, 256, sms * 16), 256, 0, st>>>(
+              dg->g, lp, P.tail_da, P.label[tail_lvl], P.tail_db, P.label[tail_lvl + 1],
+              ws->tailA, ws->tailAD);
+          res->launches++;
+          tail_ready = true;
+        } else {
+          extra_balg += ws->h_ctr[C_PROBE_BALG];
+          extra_balgc += ws->h_ctr[C_PROBE_BALGC];
+          T[lvl] = ws->h_ctr[0];
+        }
+      }
+      if (at_tail && tail_ready) {
+        // Every row is counted in closed form; nothing is expanded.
+        a.tailA = ws->tailA;
+        a.tailAD = ws->tailAD;
+        a.probe = 0;
+        k_work<<<grid_for(R[lvl], 256, sms * 16), 256, 0, st>>>(a);
+        res->launches++;
+        a.tailA = nullptr;
+        a.tailAD = nullptr;
+        T[lvl] = 0;
+      } else if (!at_tail) {
+        if ((rc = launch_work_scan(lvl, false))) return rc;
+        T[lvl] = ws->h_ctr[0];
+      }
       cur[lvl] = 0;
       need_work = false;
     }
     if (cur[lvl] < T[lvl]) {
       const uint64_t t0 = cur[lvl];
       const uint64_t t1 = writes[lvl] ? std::min(T[lvl], t0 + cap) : T[lvl];
+      a.tile_row = ws->tile_row;
       a.level = uint32_t(lvl);
       a.R = R[lvl];
       a.in = tab(lvl);
@@ -760,9 +975,16 @@ static int run_levels(DevGraph* dg, const std::vector<PlanDev>& plans, bool coun
         a.out_cap = 0;
       }
       MG_CK(cudaMemsetAsync(ws->ctr + C_OUT, 0, 8, st));
-      const unsigned blocks = grid_for(t1 - t0, EXPAND_BLOCK, sms * 8);
-      k_expand<<<blocks, EXPAND_BLOCK, 0, st>>>(a);
-      res->launches++;
+      for (uint64_t s0 = t0; s0 < t1; s0 += kSegment) {
+        const uint64_t s1 = std::min(t1, s0 + kSegment);
+        const uint32_t ntiles = uint32_t((s1 - s0 + EXPAND_BLOCK - 1) / EXPAND_BLOCK);
+        a.t0 = s0;
+        a.t1 = s1;
+        k_tile_rows<<<grid_for(uint64_t(ntiles) + 1, 256, sms * 16), 256, 0, st>>>(
+            ws->woff[lvl], R[lvl], s0, s1, ntiles, ws->tile_row);
+        k_expand<<<grid_for(s1 - s0, EXPAND_BLOCK, sms * 8), EXPAND_BLOCK, 0, st>>>(a);
+        res->launches += 2;
+      }
       res->chunks++;
       MG_CK(cudaGetLastError());
       cur[lvl] = t1;
@@ -791,8 +1013,8 @@ static int run_levels(DevGraph* dg, const std::vector<PlanDev>& plans, bool coun
   float ms = 0;
   MG_CK(cudaEventElapsedTime(&ms, ws->ev0, ws->ev1));
   res->ms = ms;
-  res->balg = ws->h_ctr[C_BALG];
-  res->balgc = ws->h_ctr[C_BALGC];
+  res->balg = ws->h_ctr[C_BALG] + extra_balg;
+  res->balgc = ws->h_ctr[C_BALGC] + extra_balgc;
   res->emitted = ws->h_ctr[C_EMIT];
   for (int i = 0; i < MAXK + 2 && C_SURV + i < C_NUM; ++i) res->surv[i] = ws->h_ctr[C_SURV + i];
   if (ws->h_ctr[C_ERR] & ERR_OVERFLOW) return set_error(MG_E_CUDA, "device table overflow");

@@ -33,8 +33,9 @@ ORDERS = {"reference": L.MG_ORDER_REFERENCE, "heuristic": L.MG_ORDER_REFERENCE,
 
 def make_opts(order="reference", filters=L.MG_FILTER_ALL, chunk_rows=0, given_order=None,
               model=None, root_range=None, mem_budget_bytes=0, persistent=0,
-              block=0, merge_min=0):
+              block=0, merge_min=0, no_tail=0):
     o = L.default_opts()
+    o.no_tail = no_tail
     o.order = ORDERS[order] if isinstance(order, str) else int(order)
     o.filters = filters
     o.chunk_rows = chunk_rows

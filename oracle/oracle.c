@@ -509,7 +509,10 @@ static int passes(const thread_ctx* T, uint32_t i, uint32_t x) {
     if (!contains(g->adj[d], lo[0], lo[1], x)) return 0;
   }
   if (P->self[i] && !g->self[x]) return 0;
-  if (i + 1 < P->k) {
+  /* Filters prune positions that are extended further, except the position
+   * before a last position with a single backward neighbour (its candidates
+   * are closed in O(1) by the slice length). */
+  if (i + 1 < P->k && !(i + 2 == P->k && P->last_o1)) {
     uint32_t f = T->S->filters;
     if (f & 1u) {
       if (g->deg[0][x] < P->req[0][i]) return 0;

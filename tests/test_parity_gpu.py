@@ -149,7 +149,7 @@ def test_batch_equals_single(c1):
     qs = [mg.query_random(g, 3 + i % 6, 0.3, seed=1000 + i) for i in range(64)]
     single = [dg.count(x) for x in qs]
     assert dg.batch_count(qs).tolist() == single
-    assert dg.batch_count(qs, chunk_rows=333).tolist() == single
+    assert dg.batch_count(qs, chunk_rows=4096).tolist() == single
     for x, c in list(zip(qs, single))[:12]:
         assert oracle_count(g, x)["count"] == c
 
@@ -177,15 +177,52 @@ def test_subiso_task_and_runtime(tmp_path, c1):
 
 
 def test_rmat_small_full_parity():
-    g = mg.rmat(14, n_labels=8, label_kind="zipf")
+    g = mg.rmat(13, n_labels=8, label_kind="zipf")
     dg = mg.DeviceGraph(g)
     og = O.Graph.from_csr(g)
     for i, shape in enumerate(mg.SHAPES):
         q = mg.query_walk(g, shape, seed=2 + i)
         want = O.count(og, O.query_from_csr(q), threads=8)
-        c, st = dg.count(q, stats=True)
-        assert c == want["count"], shape
-        assert st["level_rows"] == want["level_rows"], shape
-        assert st["balg_count_bytes"] == want["balg_count"], shape
-        assert dg.count(q, order="strong") == c
+        for tail in (0, 1, 2):
+            c, st = dg.count(q, stats=True, no_tail=tail)
+            assert c == want["count"], (shape, tail)
+            assert st["level_rows"] == want["level_rows"], (shape, tail)
+            assert st["balg_count_bytes"] == want["balg_count"], (shape, tail)
+            assert st["balg_bytes"] == want["balg"], (shape, tail)
+        assert dg.count(q, order="strong") == want["count"]
+    dg.free()
+
+
+TAIL_QUERIES = [
+    (3, [(0, 1), (1, 2)]),                          # wedge
+    (4, [(0, 1), (1, 2), (2, 3)]),                  # 4-path
+    (5, [(0, 1), (1, 2), (2, 0), (2, 3), (3, 4)]),  # triangle with a 2-tail
+    (5, [(0, 1), (0, 2), (0, 3), (3, 4)]),          # star with a 2-tail
+    (6, [(0, 1), (1, 2), (2, 3), (3, 0), (0, 4), (4, 5)]),
+]
+
+
+@pytest.mark.parametrize("seed", range(10))
+def test_tail_closed_form(seed):
+    """Closed-form pendant tails equal enumeration, incl. label collisions and
+    directed graphs with self-loops."""
+    rng = np.random.default_rng(900 + seed)
+    directed = seed % 2 == 1
+    n = int(rng.integers(10, 40))
+    edges, labels = random_graph(rng, n, 0.25, int(rng.integers(1, 3)), directed=directed,
+                                 self_loops=directed)
+    g = graph(n, edges, labels, symmetric=not directed)
+    dg = mg.DeviceGraph(g)
+    for k, qe in TAIL_QUERIES:
+        ql = rng.integers(0, max(labels) + 1, k).tolist()
+        if directed:
+            qe = [(b, a) if rng.random() < 0.5 else (a, b) for a, b in qe]
+        q = mg.CSRGraph.query(k, qe, ql, directed=directed)
+        want = oracle_count(g, q)
+        for tail in (1, 2):
+            c, st = dg.count(q, stats=True, no_tail=tail)
+            assert c == want["count"], (k, qe, ql, tail)
+            assert st["level_rows"] == want["level_rows"], (k, qe, ql, tail)
+            assert st["balg_bytes"] == want["balg"], (k, qe, ql, tail)
+            assert st["balg_count_bytes"] == want["balg_count"], (k, qe, ql, tail)
     dg.free()
