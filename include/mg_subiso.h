@@ -244,6 +244,28 @@ int  mg_subiso_batch_count_ex(void* dgraph, const mg_csr_view* const* qs,
                               uint32_t nq, const mg_opts* opts,
                               uint64_t* counts, mg_stats* st);
 
+/* Exact count that allocates nothing.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory when they ask for a count:
+ * processes whose HBM is owned by another allocator (a framework's caching
+ * allocator or a fixed arena that has reserved nearly all of it), and
+ * latency-critical paths that must not pay for cudaMalloc/cudaFree or the
+ * device-wide synchronisation cudaFree implies.  The enumeration scratch
+ * (level tables, scan space, counters, plan) lives in one file-scope device
+ * array of MG_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
+ * until the process exits; the level tables are sized to fit it, so any
+ * match count is reachable (more, smaller chunks).  A caller-set chunk_rows
+ * whose tables do not fit is rejected with MG_E_LIMIT.  The data graph must
+ * already be resident (mg_graph_upload); orders: reference, strong, given.
+ * The first call on a device looks up the array's device address with that
+ * device current; make that first call before any stream capture.  Every
+ * call shares the array and leaves its contents behind (counters are
+ * cleared at the start of each call); calls are serialised by a process-wide
+ * lock, since calls that overlapped on the GPU would race on the array.    */
+#define MG_NOALLOC_SCRATCH_BYTES (16u << 20)
+int  mg_subiso_count_noalloc(void* dgraph, const mg_csr_view* q, const mg_opts* opts,
+                             uint64_t* count);
+
 #ifdef __cplusplus
 }
 #endif

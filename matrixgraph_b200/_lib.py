@@ -128,6 +128,7 @@ _SIGS = {
                                         _PU64]),
     "mg_subiso_batch_count_ex": (C.c_int, [_VP, C.POINTER(_PV), C.c_uint32, C.POINTER(Opts),
                                            _PU64, C.POINTER(Stats)]),
+    "mg_subiso_count_noalloc": (C.c_int, [_VP, _PV, C.POINTER(Opts), _PU64]),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -1296,3 +1296,326 @@ int mg_subiso_batch_count(void* dgraph, const mg_csr_view* const* qs, uint32_t n
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free count (mg_subiso_count_noalloc)
+//
+// For callers that cannot allocate device memory when they ask for a count:
+// processes whose device memory is owned by another allocator (a framework's
+// caching allocator that has reserved nearly all HBM, a fixed arena), or
+// latency-critical paths that must not pay cudaMalloc/cudaFree and the
+// device-wide synchronisation cudaFree implies.  The level tables, scan
+// scratch, counters and the plan live in the file-scope array below, sized
+// once at load time and held by every GPU that loads the library until the
+// process exits.  The data graph must already be resident (mg_graph_upload).
+// ---------------------------------------------------------------------------
+namespace mg {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[MG_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+// Device address of g_noalloc_scratch per device, looked up once per device
+// (with that device current) by the first call on it.
+std::mutex g_noalloc_mu;  // one call at a time: every call shares the array
+void* g_noalloc_ptr[256] = {};
+
+int noalloc_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= 256) return set_error(MG_E_ARG, "device %d out of range", device);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return set_error(MG_E_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch) on device %d: %s",
+                       device, cudaGetErrorString(e));
+    g_noalloc_ptr[device] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_ptr[device]);
+  return MG_OK;
+}
+
+// Carves the level tables of a single-query count out of `base`; returns the
+// bytes used (a size above MG_NOALLOC_SCRATCH_BYTES means it does not fit).
+struct NoallocLayout {
+  unsigned long long* ctr;
+  unsigned long long* counts;
+  PlanDev* plan;
+  uint64_t* bsum;
+  uint32_t* tile_row;
+  uint32_t* col[MAXK][MAXK];
+  uint32_t* work[MAXK];
+  uint64_t* woff[MAXK];
+  uint32_t* dstart[MAXK];
+  uint8_t* dci[MAXK];
+};
+
+// Elements per expand launch of a level whose survivors are not stored.
+constexpr uint64_t kNoallocSegment = 1ull << 24;
+
+uint64_t noalloc_carve(unsigned char* base, uint64_t cap, uint32_t k, NoallocLayout* L) {
+  uint64_t off = 0;
+  auto take = [&](uint64_t bytes) -> unsigned char* {
+    off = (off + 255) & ~uint64_t(255);
+    unsigned char* p = base ? base + off : nullptr;
+    off += bytes;
+    return p;
+  };
+  L->ctr = reinterpret_cast<unsigned long long*>(take(C_NUM * 8));
+  L->counts = reinterpret_cast<unsigned long long*>(take(8));
+  L->plan = reinterpret_cast<PlanDev*>(take(sizeof(PlanDev)));
+  L->bsum = reinterpret_cast<uint64_t*>(take((cap / SCAN_TILE + 2) * 8));
+  L->tile_row = reinterpret_cast<uint32_t*>(take((kNoallocSegment / EXPAND_BLOCK + 2) * 4));
+  for (uint32_t l = 0; l < k; ++l) {
+    const uint64_t rows = l == 0 ? 1 : cap;
+    for (uint32_t j = 0; j < l; ++j) L->col[l][j] = reinterpret_cast<uint32_t*>(take(rows * 4));
+    L->work[l] = reinterpret_cast<uint32_t*>(take(rows * 4));
+    L->woff[l] = reinterpret_cast<uint64_t*>(take((rows + 1) * 8));
+    L->dstart[l] = reinterpret_cast<uint32_t*>(take(rows * 4));
+    L->dci[l] = reinterpret_cast<uint8_t*>(take(rows));
+  }
+  return off;
+}
+
+// Query normalisation into fixed-size storage (no heap): labels, edge masks
+// and the directed edges in CSR order.
+int noalloc_query(const mg_csr_view* q, QueryGraph* Q, uint32_t (*edges)[2], uint32_t* ne) {
+  int rc = validate_csr_view(q);
+  if (rc) return rc;
+  if (q->n == 0) return set_error(MG_E_ARG, "empty query");
+  if (q->n > MG_MAX_QUERY_VERTICES)
+    return set_error(MG_E_LIMIT, "query has %u vertices; at most %d supported", q->n,
+                     MG_MAX_QUERY_VERTICES);
+  Q->k = q->n;
+  *ne = 0;
+  for (uint32_t i = 0; i < q->n; ++i) {
+    Q->label_raw[i] = q->labels[i];
+    Q->out_mask[i] = Q->in_mask[i] = 0;
+    for (uint32_t j = 0; j < i; ++j)
+      if (q->globalid[j] == q->globalid[i])
+        return set_error(MG_E_FORMAT, "query globalid %u repeated", q->globalid[i]);
+  }
+  for (uint32_t u = 0; u < q->n; ++u)
+    for (uint32_t e = q->out_off[u]; e < q->out_off[u + 1]; ++e) {
+      uint32_t w = FULL;
+      for (uint32_t x = 0; x < q->n; ++x)
+        if (q->globalid[x] == q->out_edges[e]) w = x;
+      if (w == FULL)
+        return set_error(MG_E_FORMAT, "query out-edge to unknown vertex %u", q->out_edges[e]);
+      if (!((Q->out_mask[u] >> w) & 1u)) {
+        edges[*ne][0] = u;
+        edges[*ne][1] = w;
+        ++*ne;
+      }
+      Q->out_mask[u] |= 1u << w;
+      Q->in_mask[w] |= 1u << u;
+    }
+  return MG_OK;
+}
+
+// The reference vertex-introduction order over a fixed edge array (same rule
+// as order_reference).
+void noalloc_order_reference(uint32_t k, const uint32_t (*edges)[2], uint32_t ne,
+                             uint32_t* order) {
+  uint32_t placed = 0, n = 0;
+  auto place = [&](uint32_t v) {
+    if (!((placed >> v) & 1u)) {
+      placed |= 1u << v;
+      order[n++] = v;
+    }
+  };
+  if (ne) {
+    place(edges[0][0]);
+    place(edges[0][1]);
+  }
+  while (n < k) {
+    bool changed = true;
+    while (changed) {
+      changed = false;
+      for (uint32_t e = 0; e < ne; ++e) {
+        const bool a = (placed >> edges[e][0]) & 1u, b = (placed >> edges[e][1]) & 1u;
+        if (a && !b) {
+          place(edges[e][1]);
+          changed = true;
+        } else if (b && !a) {
+          place(edges[e][0]);
+          changed = true;
+        }
+      }
+    }
+    for (uint32_t v = 0; v < k && n < k; ++v)
+      if (!((placed >> v) & 1u)) {
+        place(v);
+        break;
+      }
+  }
+}
+
+int noalloc_count(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint64_t* count) {
+  mg_opts o;
+  mg_opts_default(&o);
+  if (opts) o = *opts;
+  QueryGraph Q;
+  uint32_t edges[MAXK * MAXK][2];
+  uint32_t ne = 0;
+  int rc = noalloc_query(q, &Q, edges, &ne);
+  if (rc) return rc;
+  uint32_t order[MAXK];
+  if (o.order == MG_ORDER_REFERENCE) {
+    noalloc_order_reference(Q.k, edges, ne, order);
+  } else if (o.order == MG_ORDER_STRONG) {
+    order_strong(Q, dg->stats, order);
+  } else if (o.order == MG_ORDER_GIVEN) {
+    if (!o.given_order) return set_error(MG_E_ARG, "MG_ORDER_GIVEN without given_order");
+    std::memcpy(order, o.given_order, Q.k * 4);
+    if (!order_is_permutation(order, Q.k))
+      return set_error(MG_E_ARG, "given_order is not a permutation of 0..%u", Q.k - 1);
+  } else {
+    return set_error(MG_E_ARG, "mg_subiso_count_noalloc supports the reference, strong and "
+                               "given orders only");
+  }
+  PlanDev P;
+  if ((rc = build_plan(dg, Q, order, &P))) return rc;
+  const uint32_t k = P.k;
+
+  // Rows per level table: the largest power of two whose layout fits, or the
+  // caller's chunk_rows, which must fit.
+  NoallocLayout L;
+  uint64_t cap = 0;
+  if (o.chunk_rows) {
+    if (o.chunk_rows > (1ull << 31) ||
+        noalloc_carve(nullptr, o.chunk_rows, k, &L) > MG_NOALLOC_SCRATCH_BYTES)
+      return set_error(MG_E_LIMIT,
+                       "chunk_rows=%llu for a %u-vertex query needs %llu bytes of scratch; the "
+                       "static scratch holds %llu bytes",
+                       (unsigned long long)o.chunk_rows, k,
+                       (unsigned long long)noalloc_carve(nullptr, std::min<uint64_t>(
+                           o.chunk_rows, 1ull << 31), k, &L),
+                       (unsigned long long)MG_NOALLOC_SCRATCH_BYTES);
+    cap = o.chunk_rows;
+  } else {
+    for (uint64_t c = 1ull << 22; c >= 64; c >>= 1)
+      if (noalloc_carve(nullptr, c, k, &L) <= MG_NOALLOC_SCRATCH_BYTES) {
+        cap = c;
+        break;
+      }
+    if (!cap)
+      return set_error(MG_E_LIMIT, "a %u-vertex query does not fit the %llu-byte static scratch",
+                       k, (unsigned long long)MG_NOALLOC_SCRATCH_BYTES);
+  }
+  unsigned char* base = nullptr;
+  if ((rc = noalloc_scratch(dg->device, &base))) return rc;
+  noalloc_carve(base, cap, k, &L);
+
+  cudaStream_t st = dg->stream;
+  // The array keeps the previous call's contents: counters start at zero.
+  MG_CK(cudaMemcpyAsync(L.plan, &P, sizeof(PlanDev), cudaMemcpyHostToDevice, st));
+  MG_CK(cudaMemsetAsync(L.counts, 0, 8, st));
+  MG_CK(cudaMemsetAsync(L.ctr, 0, C_NUM * 8, st));
+
+  StepArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.g = dg->g;
+  a.plans = L.plan;
+  a.ctr = L.ctr;
+  a.counts = L.counts;
+  a.count_mode = 1;
+  a.filters = o.filters & MG_FILTER_ALL;
+  a.nq = 1;
+  a.tile_row = L.tile_row;
+  if (o.root_end) {
+    if (o.root_begin > o.root_end) return set_error(MG_E_ARG, "root_begin > root_end");
+    a.root_begin = o.root_begin;
+    a.root_end = o.root_end;
+  }
+  bool writes[MAXK] = {};
+  for (uint32_t l = 0; l < k; ++l)
+    writes[l] = P.k > l + 1 && !(P.k == l + 2 && P.last_o1);
+  auto tab = [&](uint32_t l) {
+    TabPtrs t{};
+    for (uint32_t j = 0; j < l; ++j) t.col[j] = L.col[l][j];
+    return t;
+  };
+  const unsigned sms = 148;
+  uint64_t T[MAXK] = {}, cur[MAXK] = {}, host_u64 = 0;
+  uint32_t R[MAXK] = {};
+  R[0] = 1;
+  int lvl = 0;
+  bool need_work = true;
+  while (true) {
+    a.level = uint32_t(lvl);
+    a.R = R[lvl];
+    a.in = tab(lvl);
+    a.work = L.work[lvl];
+    a.woff = L.woff[lvl];
+    a.dstart = L.dstart[lvl];
+    a.dci = L.dci[lvl];
+    if (need_work) {
+      k_work<<<grid_for(R[lvl], 256, sms * 16), 256, 0, st>>>(a);
+      const uint32_t nb = (R[lvl] + SCAN_TILE - 1) / SCAN_TILE;
+      k_scan_reduce<<<nb, 256, 0, st>>>(L.work[lvl], R[lvl], L.bsum);
+      k_scan_bsum<<<1, 1024, 0, st>>>(L.bsum, nb, L.woff[lvl] + R[lvl]);
+      k_scan_apply<<<nb, 256, 0, st>>>(L.work[lvl], R[lvl], L.bsum, L.woff[lvl]);
+      MG_CK(cudaMemcpyAsync(&host_u64, L.woff[lvl] + R[lvl], 8, cudaMemcpyDeviceToHost, st));
+      MG_CK(cudaStreamSynchronize(st));
+      T[lvl] = host_u64;
+      cur[lvl] = 0;
+      need_work = false;
+    }
+    if (cur[lvl] < T[lvl]) {
+      const uint64_t t0 = cur[lvl];
+      const uint64_t t1 = writes[lvl] ? std::min(T[lvl], t0 + cap) : T[lvl];
+      a.out = writes[lvl] ? tab(lvl + 1) : TabPtrs{};
+      a.out_cap = writes[lvl] ? cap : 0;
+      MG_CK(cudaMemsetAsync(L.ctr + C_OUT, 0, 8, st));
+      const uint64_t seg = writes[lvl] ? std::min<uint64_t>(cap, kNoallocSegment) : kNoallocSegment;
+      for (uint64_t s0 = t0; s0 < t1; s0 += seg) {
+        const uint64_t s1 = std::min(t1, s0 + seg);
+        const uint32_t ntiles = uint32_t((s1 - s0 + EXPAND_BLOCK - 1) / EXPAND_BLOCK);
+        a.t0 = s0;
+        a.t1 = s1;
+        k_tile_rows<<<grid_for(uint64_t(ntiles) + 1, 256, sms * 16), 256, 0, st>>>(
+            L.woff[lvl], R[lvl], s0, s1, ntiles, L.tile_row);
+        k_expand<<<grid_for(s1 - s0, EXPAND_BLOCK, sms * 8), EXPAND_BLOCK, 0, st>>>(a);
+      }
+      MG_CK(cudaGetLastError());
+      cur[lvl] = t1;
+      if (writes[lvl]) {
+        MG_CK(cudaMemcpyAsync(&host_u64, L.ctr + C_OUT, 8, cudaMemcpyDeviceToHost, st));
+        MG_CK(cudaStreamSynchronize(st));
+        if (host_u64 > cap)
+          return set_error(MG_E_CUDA, "level table overflow (%llu > %llu)",
+                           (unsigned long long)host_u64, (unsigned long long)cap);
+        if (host_u64 > 0) {
+          R[lvl + 1] = uint32_t(host_u64);
+          ++lvl;
+          need_work = true;
+        }
+      }
+    } else {
+      if (lvl == 0) break;
+      --lvl;
+    }
+  }
+  unsigned long long err = 0, c = 0;
+  MG_CK(cudaMemcpyAsync(&err, L.ctr + C_ERR, 8, cudaMemcpyDeviceToHost, st));
+  MG_CK(cudaMemcpyAsync(&c, L.counts, 8, cudaMemcpyDeviceToHost, st));
+  MG_CK(cudaStreamSynchronize(st));
+  MG_CK(cudaGetLastError());
+  if (err & ERR_OVERFLOW) return set_error(MG_E_CUDA, "device table overflow");
+  *count = c;
+  return MG_OK;
+}
+
+}  // namespace
+}  // namespace mg
+
+extern "C" int mg_subiso_count_noalloc(void* dgraph, const mg_csr_view* q, const mg_opts* opts,
+                                       uint64_t* count) {
+  mg::clear_error();
+  if (!dgraph || !q || !count) return mg::set_error(MG_E_ARG, "null argument");
+  auto* dg = static_cast<mg::DevGraph*>(dgraph);
+  std::lock_guard<std::mutex> glock(mg::g_noalloc_mu);
+  std::lock_guard<std::mutex> lock(dg->mu);
+  mg::DeviceGuard guard(dg->device);
+  return mg::noalloc_count(dg, q, opts, count);
+}
