@@ -93,18 +93,22 @@ typedef struct mg_opts {
   void*    model;            /* order model for MG_ORDER_LEARNED (may be NULL:
                                 then the reference order is used)            */
   uint64_t chunk_rows;       /* partial-match rows per level chunk; 0 = auto */
-  uint32_t block;            /* threads per block of the expand kernel; 0=auto */
-  uint32_t merge_min;        /* warp-merge intersection when the other list's
-                                covered window <= merge_min*32; 0 = auto     */
+  uint32_t grab;             /* expand tiles (256 candidates each) a block
+                                takes from the device work queue at a time;
+                                0 = auto                                     */
+  uint32_t merge_min;        /* reserved, 0                                  */
   uint32_t spin_limit;       /* iteration cap of device waits; 0 = default   */
   uint32_t persistent;       /* 1: one persistent launch drives all levels  */
   uint64_t mem_budget_bytes; /* cap on enumeration scratch; 0 = auto        */
   uint64_t root_begin;       /* level-0 candidates [root_begin, root_end) of  */
   uint64_t root_end;         /* the first position's label bucket; 0,0 = all  */
   uint32_t no_tail;          /* closed-form count of a two-position pendant
-                                tail (count mode): 0 = when it pays off,
-                                1 = never, 2 = always                        */
+                                tail (count mode): 0 or 2 = whenever the plan
+                                ends in one, 1 = never                       */
   uint32_t _reserved;
+  uint64_t max_elements;     /* work budget: candidate elements expanded by
+                                one call; above it the call returns
+                                MG_E_LIMIT (0 = unlimited)                   */
 } mg_opts;
 
 /* Per-call statistics (optional out-parameter of the *_ex entry points). */
@@ -118,6 +122,7 @@ typedef struct mg_stats {
   double   device_ms;        /* device time from first launch to result      */
   uint64_t launches;         /* kernels launched by this call                */
   uint64_t chunks;           /* level chunks processed                       */
+  uint64_t elements;         /* candidate elements expanded                  */
 } mg_stats;
 
 typedef struct mg_graph_info {

@@ -57,18 +57,20 @@ class CsrView(C.Structure):
 
 class Opts(C.Structure):
     _fields_ = [("order", C.c_int32), ("filters", C.c_uint32), ("given_order", P32),
-                ("model", C.c_void_p), ("chunk_rows", C.c_uint64), ("block", C.c_uint32),
+                ("model", C.c_void_p), ("chunk_rows", C.c_uint64), ("grab", C.c_uint32),
                 ("merge_min", C.c_uint32), ("spin_limit", C.c_uint32),
                 ("persistent", C.c_uint32), ("mem_budget_bytes", C.c_uint64),
                 ("root_begin", C.c_uint64), ("root_end", C.c_uint64),
-                ("no_tail", C.c_uint32), ("_reserved", C.c_uint32)]
+                ("no_tail", C.c_uint32), ("_reserved", C.c_uint32),
+                ("max_elements", C.c_uint64)]
 
 
 class Stats(C.Structure):
     _fields_ = [("k", C.c_uint32), ("order", C.c_uint32 * MG_MAX_QUERY_VERTICES),
                 ("level_rows", C.c_uint64 * (MG_MAX_QUERY_VERTICES + 1)),
                 ("balg_bytes", C.c_uint64), ("balg_count_bytes", C.c_uint64),
-                ("device_ms", C.c_double), ("launches", C.c_uint64), ("chunks", C.c_uint64)]
+                ("device_ms", C.c_double), ("launches", C.c_uint64), ("chunks", C.c_uint64),
+                ("elements", C.c_uint64)]
 
 
 class GraphInfo(C.Structure):

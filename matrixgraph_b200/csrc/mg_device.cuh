@@ -68,6 +68,14 @@ struct PlanDev {
   uint32_t tail_p, tail_da, tail_db;
   uint32_t tail_Ia;  // positions i < a labelled like position a
   uint32_t tail_J;   // positions j < a labelled like position b
+  uint32_t tail_kid; // index of (da, la, db, lb) in the call's tail-key table
+};
+
+// Signature of a two-hop aggregate: A(y) = sum over the da-slice of y labelled
+// la of the db-slice lengths labelled lb.  Queries sharing a signature share
+// memoised aggregates.
+struct TailKey {
+  uint32_t da, la, db, lb;
 };
 
 struct Workspace;  // enumeration scratch (mg_enum.cu)

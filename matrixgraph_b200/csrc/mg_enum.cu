@@ -52,8 +52,15 @@ struct Workspace {
   uint64_t* bsum = nullptr;
   uint32_t bsum_cap = 0;
   uint32_t* tile_row = nullptr;  // first row of every expand tile of a segment
-  unsigned long long* tailA = nullptr;   // per-vertex two-hop aggregates (n each)
-  unsigned long long* tailAD = nullptr;
+  // Memoised two-hop aggregates: open-addressing table keyed by
+  // (tail key id << 32 | vertex), values A and AD, list of new slots.
+  uint64_t* hkeys = nullptr;
+  unsigned long long* hA = nullptr;
+  unsigned long long* hAD = nullptr;
+  uint32_t* hnew = nullptr;
+  uint64_t hsize = 0;
+  TailKey* tkeys = nullptr;
+  uint32_t tkeys_cap = 0;
   unsigned long long* ctr = nullptr;     // device counters
   unsigned long long* h_ctr = nullptr;   // pinned mirror
   unsigned long long* counts = nullptr;  // per query
@@ -67,8 +74,8 @@ struct Workspace {
 
 // Counter slots.
 enum : int {
-  C_OUT = 0, C_BALG = 1, C_BALGC = 2, C_ERR = 3, C_EMIT = 4, C_PROBE_BALG = 5,
-  C_PROBE_BALGC = 6, C_SURV = 8, C_NUM = 8 + MAXK + 2
+  C_OUT = 0, C_BALG = 1, C_BALGC = 2, C_ERR = 3, C_EMIT = 4, C_HNEW = 5, C_TILE = 6, C_SURV = 8,
+  C_NUM = 8 + MAXK + 2
 };
 
 void free_workspace(Workspace* ws) {
@@ -174,9 +181,15 @@ struct StepArgs {
   uint64_t emit_cap;
   uint64_t root_begin, root_end;  // level-0 candidate range (root_end 0: all)
   const uint32_t* tile_row;        // first row of each tile of [t0, t1)
-  const unsigned long long* tailA;  // non-null: count tail rows in closed form
-  const unsigned long long* tailAD;
-  uint32_t probe;                   // charge algorithmic bytes to the probe slots
+  // Pendant tails counted in closed form (tail_on): memo table of aggregates.
+  uint32_t grab;   // expand tiles taken per work-queue grab
+  uint32_t tail_on;
+  uint64_t* hkeys;
+  unsigned long long* hA;
+  unsigned long long* hAD;
+  uint32_t* hnew;
+  uint64_t hmask;
+  const TailKey* tkeys;
 };
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -240,6 +253,95 @@ __device__ __forceinline__ uint32_t find_row(const uint64_t* __restrict__ woff, 
   return lo;
 }
 
+// Memo table of two-hop aggregates (open addressing, linear probing).  The
+// host keeps the load at or below one half, so probing always ends.
+constexpr uint64_t MEMO_EMPTY = ~0ull;
+
+__device__ __forceinline__ uint64_t memo_hash(uint64_t key) {
+  key ^= key >> 33;
+  key *= 0xff51afd7ed558ccdull;
+  key ^= key >> 33;
+  key *= 0xc4ceb9fe1a85ec53ull;
+  key ^= key >> 33;
+  return key;
+}
+
+__device__ __forceinline__ uint64_t memo_find(const StepArgs& a, uint64_t key) {
+  uint64_t slot = memo_hash(key) & a.hmask;
+  for (uint64_t probe = 0; probe <= a.hmask; ++probe) {
+    const uint64_t k = a.hkeys[slot];
+    if (k == key || k == MEMO_EMPTY) break;
+    slot = (slot + 1) & a.hmask;
+  }
+  return slot;
+}
+
+__device__ __forceinline__ bool tail_row(const StepArgs& a, const PlanDev& P) {
+  return a.tail_on && P.tail2 && a.level + 2 == P.k;
+}
+
+// Inserts (tail key, m_p) of every tail row; new slots are listed in hnew.
+__global__ void __launch_bounds__(256) k_tail_collect(StepArgs a) {
+  for (uint64_t r = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; r < a.R;
+       r += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t q = a.in.qid ? a.in.qid[r] : 0u;
+    const PlanDev& P = a.plans[q];
+    if (!tail_row(a, P)) continue;
+    const uint64_t key = (uint64_t(P.tail_kid) << 32) | a.in.col[P.tail_p][r];
+    uint64_t slot = memo_hash(key) & a.hmask;
+    for (uint64_t probe = 0; probe <= a.hmask; ++probe) {
+      const uint64_t seen = a.hkeys[slot];  // plain probe first: most keys exist
+      if (seen == key) break;
+      if (seen != MEMO_EMPTY) {
+        slot = (slot + 1) & a.hmask;
+        continue;
+      }
+      const unsigned long long old = atomicCAS(
+          reinterpret_cast<unsigned long long*>(a.hkeys + slot), MEMO_EMPTY, key);
+      if (old == MEMO_EMPTY) {
+        const unsigned long long idx = atomicAdd(&a.ctr[C_HNEW], 1ull);
+        a.hnew[idx] = uint32_t(slot);
+        break;
+      }
+      if (old == key) break;
+      slot = (slot + 1) & a.hmask;
+    }
+  }
+}
+
+// Aggregates of the new slots, warp per slot:
+// A(y) = sum_{x in N^{da}_{la}(y)} (|N^{db}_{lb}(x)| - [x self-loop, la == lb]),
+// AD(y) = sum_{x in N^{da}_{la}(y)} |N^{db}_{lb}(x)|.
+__global__ void __launch_bounds__(256) k_tail_compute(StepArgs a, uint64_t first) {
+  const GraphDev& g = a.g;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5;
+  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  const uint64_t total = a.ctr[C_HNEW];
+  for (uint64_t w = first + warp; w < total; w += nwarps) {
+    const uint32_t slot = a.hnew[w];
+    const uint64_t key = a.hkeys[slot];
+    const TailKey tk = a.tkeys[key >> 32];
+    const uint32_t y = uint32_t(key);
+    uint32_t s, e;
+    slice_of(g, tk.da, y, tk.la, s, e);
+    unsigned long long sa = 0, sd = 0;
+    for (uint32_t j = s + lane; j < e; j += 32) {
+      const uint32_t x = __ldg(g.adj[tk.da] + j);
+      uint32_t xs, xe;
+      slice_of(g, tk.db, x, tk.lb, xs, xe);
+      sd += xe - xs;
+      sa += xe - xs - ((tk.la == tk.lb && has_self(g, x)) ? 1u : 0u);
+    }
+    sa = warp_sum(sa);
+    sd = warp_sum(sd);
+    if (lane == 0) {
+      a.hA[slot] = sa;
+      a.hAD[slot] = sd;
+    }
+  }
+}
+
 // Work kernel: per row, the driving slice (shortest backward slice, or the
 // label bucket for a position without backward neighbours) and the
 // algorithmic-byte charge of extending the row.
@@ -261,8 +363,9 @@ __device__ __forceinline__ void tail_count(const StepArgs& a, const PlanDev& P, 
   const uint32_t mp = a.in.col[P.tail_p][r];
   uint32_t s, e;
   slice_of(g, da, mp, la, s, e);
-  long long c = (long long)a.tailA[mp];
-  long long d = (long long)a.tailAD[mp];
+  const uint64_t slot = memo_find(a, (uint64_t(P.tail_kid) << 32) | mp);
+  long long c = (long long)a.hA[slot];
+  long long d = (long long)a.hAD[slot];
   unsigned long long inS = 0;
   for (uint32_t mi = P.tail_Ia; mi; mi &= mi - 1) {
     const uint32_t i2 = __ffs(mi) - 1;
@@ -288,10 +391,15 @@ __device__ __forceinline__ void tail_count(const StepArgs& a, const PlanDev& P, 
 
 __global__ void __launch_bounds__(256) k_work(StepArgs a) {
   unsigned long long bal = 0, balc = 0, tcnt = 0, tpre = 0;
+  uint32_t tq = 0;
   const uint32_t i = a.level;
   const GraphDev& g = a.g;
-  for (uint64_t r = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; r < a.R;
-       r += uint64_t(gridDim.x) * blockDim.x) {
+  // Contiguous rows per block: rows of one query stay together, so the
+  // per-thread tail-count accumulator rarely changes query.
+  const uint64_t per = ((a.R + gridDim.x - 1) / gridDim.x + blockDim.x - 1) / blockDim.x *
+                       blockDim.x;
+  const uint64_t r_end = min(uint64_t(a.R), (uint64_t(blockIdx.x) + 1) * per);
+  for (uint64_t r = blockIdx.x * per + threadIdx.x; r < r_end; r += blockDim.x) {
     const uint32_t q = a.in.qid ? a.in.qid[r] : 0u;
     const PlanDev& P = a.plans[q];
     const uint32_t lab = P.label[i];
@@ -299,7 +407,7 @@ __global__ void __launch_bounds__(256) k_work(StepArgs a) {
     uint32_t best, bs = 0;
     uint8_t bci = DCI_BUCKET;
     unsigned long long ch = 0, chc = 0;
-    if (a.tailA && P.tail2 && i + 2 == P.k) {
+    if (tail_row(a, P)) {
       // position a = k-2: one backward slice; position b counted in closed form
       const uint32_t cs = P.cons[i][0];
       uint32_t s, e;
@@ -308,6 +416,11 @@ __global__ void __launch_bounds__(256) k_work(StepArgs a) {
       tail_count(a, P, r, cnt, pre, dsum);
       ch = 8ull + 4ull * (e - s) + 8ull * pre + 4ull * dsum;
       chc = 8ull + 4ull * (e - s) + 8ull * pre;
+      if (q != tq) {
+        if (tcnt) atomicAdd(&a.counts[tq], tcnt);
+        tcnt = 0;
+        tq = q;
+      }
       tcnt += cnt;
       tpre += pre;
       a.work[r] = 0;
@@ -354,48 +467,23 @@ __global__ void __launch_bounds__(256) k_work(StepArgs a) {
   bal = warp_sum(bal);
   balc = warp_sum(balc);
   if ((threadIdx.x & 31) == 0 && (bal | balc)) {
-    atomicAdd(&a.ctr[a.probe ? C_PROBE_BALG : C_BALG], bal);
-    atomicAdd(&a.ctr[a.probe ? C_PROBE_BALGC : C_BALGC], balc);
+    atomicAdd(&a.ctr[C_BALG], bal);
+    atomicAdd(&a.ctr[C_BALGC], balc);
   }
-  if (a.tailA) {  // single-query mode only
-    tcnt = warp_sum(tcnt);
-    tpre = warp_sum(tpre);
-    if ((threadIdx.x & 31) == 0) {
-      if (tcnt) atomicAdd(&a.counts[0], tcnt);
-      if (a.stats && tpre) atomicAdd(&a.ctr[C_SURV + i + 1], tpre);
-      if (a.stats && tcnt) atomicAdd(&a.ctr[C_SURV + i + 2], tcnt);
+  if (a.tail_on) {
+    if (a.stats) {  // single query: P_{k-1} and P_k of the tail rows
+      unsigned long long sp = warp_sum(tpre), sc = warp_sum(tcnt);
+      if ((threadIdx.x & 31) == 0) {
+        if (sp) atomicAdd(&a.ctr[C_SURV + i + 1], sp);
+        if (sc) atomicAdd(&a.ctr[C_SURV + i + 2], sc);
+      }
     }
-  }
-}
-
-// Two-hop aggregates over the label bucket of position p's label:
-// A(y) = sum_{x in N^{da}_{la}(y)} (|N^{db}_{lb}(x)| - [x self-loop, la == lb]),
-// AD(y) = sum_{x in N^{da}_{la}(y)} |N^{db}_{lb}(x)|.  Warp per vertex.
-__global__ void __launch_bounds__(256) k_tail_aggregate(GraphDev g, uint32_t bucket_lab,
-                                                        uint32_t da, uint32_t la, uint32_t db,
-                                                        uint32_t lb, unsigned long long* A,
-                                                        unsigned long long* AD) {
-  const uint32_t lane = threadIdx.x & 31;
-  const uint64_t warp = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5;
-  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-  const uint32_t b0 = g.bucket_off[bucket_lab], b1 = g.bucket_off[bucket_lab + 1];
-  for (uint64_t w = warp; w < b1 - b0; w += nwarps) {
-    const uint32_t y = g.bucket_vid[b0 + w];
-    uint32_t s, e;
-    slice_of(g, da, y, la, s, e);
-    unsigned long long sa = 0, sd = 0;
-    for (uint32_t j = s + lane; j < e; j += 32) {
-      const uint32_t x = __ldg(g.adj[da] + j);
-      uint32_t xs, xe;
-      slice_of(g, db, x, lb, xs, xe);
-      sd += xe - xs;
-      sa += xe - xs - ((la == lb && has_self(g, x)) ? 1u : 0u);
-    }
-    sa = warp_sum(sa);
-    sd = warp_sum(sd);
-    if (lane == 0) {
-      A[y] = sa;
-      AD[y] = sd;
+    const uint32_t same = __match_any_sync(FULL, tq);
+    if (same == FULL) {
+      const unsigned long long sc = warp_sum(tcnt);
+      if ((threadIdx.x & 31) == 0 && sc) atomicAdd(&a.counts[tq], sc);
+    } else if (tcnt) {
+      atomicAdd(&a.counts[tq], tcnt);
     }
   }
 }
@@ -511,7 +599,20 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
   const uint64_t ntiles = (span + EXPAND_BLOCK - 1) / EXPAND_BLOCK;
   unsigned long long cnt = 0, bal = 0, balc = 0, surv1 = 0, survk = 0;
   uint32_t cnt_q = 0;
-  for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  // Device work queue: each block takes `grab` consecutive tiles at a time,
+  // so a block walks contiguous element ranges (same rows, same query) and a
+  // hub row's elements still spread over many blocks.
+  __shared__ unsigned long long s_base, s_wbase;
+  __shared__ uint32_t s_wcnt[EXPAND_BLOCK / 32];
+  const uint64_t grab = a.grab ? a.grab : 4;
+  for (;;) {
+  if (threadIdx.x == 0) s_base = atomicAdd(&a.ctr[C_TILE], (unsigned long long)grab);
+  __syncthreads();
+  const uint64_t gbase = s_base;
+  __syncthreads();
+  if (gbase >= ntiles) break;
+  const uint64_t gend = min(gbase + grab, ntiles);
+  for (uint64_t tile = gbase; tile < gend; ++tile) {
     const uint64_t tb = a.t0 + tile * EXPAND_BLOCK;
     const uint64_t te = min(tb + EXPAND_BLOCK, a.t1);
     const uint32_t rlo = __ldg(a.tile_row + tile), rhi = __ldg(a.tile_row + tile + 1);
@@ -598,16 +699,26 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
         }
       }
     }
-    // Survivors that extend the prefix: append to the next level table.
+    // Survivors that extend the prefix: append to the next level table.  One
+    // reservation per tile keeps a tile's survivors (one row run, usually one
+    // query) contiguous in the next table.
     const bool wr = ok && !fin && !fused;
     const uint32_t wm = __ballot_sync(FULL, wr);
+    if (lane == 0) s_wcnt[threadIdx.x >> 5] = __popc(wm);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t tot = 0;
+      for (uint32_t w = 0; w < EXPAND_BLOCK / 32; ++w) {
+        const uint32_t c = s_wcnt[w];
+        s_wcnt[w] = tot;
+        tot += c;
+      }
+      s_wbase = tot ? atomicAdd(&a.ctr[C_OUT], (unsigned long long)tot) : 0ull;
+    }
+    __syncthreads();
     if (wm) {
-      const uint32_t leader = __ffs(wm) - 1;
-      unsigned long long base = 0;
-      if (lane == leader) base = atomicAdd(&a.ctr[C_OUT], (unsigned long long)__popc(wm));
-      base = __shfl_sync(FULL, base, leader);
       if (wr) {
-        const unsigned long long idx = base + __popc(wm & lanemask_lt());
+        const unsigned long long idx = s_wbase + s_wcnt[threadIdx.x >> 5] + __popc(wm & lanemask_lt());
         if (idx < a.out_cap) {
           for (uint32_t j = 0; j < i; ++j) a.out.col[j][idx] = a.in.col[j][r];
           a.out.col[i][idx] = x;
@@ -637,7 +748,15 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
         }
       }
     }
+    __syncthreads();  // s_wcnt / s_wbase are reused by the next tile
   }
+  // Once per grab: fold the per-thread counts of a warp that holds one query.
+  if (__all_sync(FULL, cnt_q == __shfl_sync(FULL, cnt_q, 0))) {
+    const unsigned long long sc = warp_sum(cnt);
+    if (lane == 0 && sc) atomicAdd(&a.counts[cnt_q], sc);
+    cnt = 0;
+  }
+  }  // grab loop
   // Flush per-thread counts: warp-reduce when the whole warp holds one query.
   const uint32_t same = __match_any_sync(FULL, cnt_q);
   if (same == FULL) {
@@ -787,7 +906,7 @@ struct EmitBuf {
 };
 
 struct RunResult {
-  uint64_t balg = 0, balgc = 0, launches = 0, chunks = 0;
+  uint64_t balg = 0, balgc = 0, launches = 0, chunks = 0, elements = 0;
   uint64_t surv[MAXK + 2] = {};
   uint64_t emitted = 0;
   double ms = 0;
@@ -798,7 +917,7 @@ static inline unsigned grid_for(uint64_t items, unsigned block, unsigned cap) {
   return unsigned(std::max<uint64_t>(1, std::min<uint64_t>(g, cap)));
 }
 
-static int run_levels(DevGraph* dg, const std::vector<PlanDev>& plans, bool count_mode,
+static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
                       const EmitBuf* emit, const mg_opts& o, uint64_t* counts_out,
                       RunResult* res) {
   const uint32_t nq = uint32_t(plans.size());
@@ -843,6 +962,7 @@ static int run_levels(DevGraph* dg, const std::vector<PlanDev>& plans, bool coun
   a.counts = ws->counts;
   a.count_mode = count_mode ? 1u : 0u;
   a.filters = o.filters & MG_FILTER_ALL;
+  a.grab = o.grab;
   a.stats = nq == 1 ? 1u : 0u;
   a.nq = nq;
   if (emit) {
@@ -865,23 +985,64 @@ static int run_levels(DevGraph* dg, const std::vector<PlanDev>& plans, bool coun
   int lvl = 0;
   bool need_work = true;
   const unsigned sms = 148;
+  uint64_t elements = 0;
 
-  // Closed-form two-position tail (single query, count mode): enabled once
-  // the elements met at position k-2 outweigh the one-off aggregate pass.
-  const bool tail_possible = count_mode && nq == 1 && plans[0].tail2 && o.no_tail != 1;
-  const bool tail_forced = o.no_tail == 2;
-  const int tail_lvl = int(plans[0].k) - 2;
-  bool tail_ready = false;
-  uint64_t tail_T = 0, tail_cost = 0, extra_balg = 0, extra_balgc = 0;
-  if (tail_possible) {
-    if ((rc = ensure_full_stats(dg))) return rc;
-    const PlanDev& P = plans[0];
-    const uint32_t lp = P.label[P.tail_p], la = P.label[tail_lvl], L = dg->g.L;
-    tail_cost = P.tail_da == 0 ? dg->stats.label_pair_edges[uint64_t(lp) * L + la]
-                               : dg->stats.label_pair_edges[uint64_t(la) * L + lp];
+  // Pendant tails counted in closed form (count mode): tail-key table and
+  // memo table of two-hop aggregates, shared by every query of the call.
+  uint32_t tail_levels = 0;
+  if (count_mode && o.no_tail != 1) {
+    std::vector<TailKey> keys;
+    for (PlanDev& p : plans) {
+      if (!p.tail2) continue;
+      const TailKey tk{p.tail_da, p.label[p.k - 2], p.tail_db, p.label[p.k - 1]};
+      uint32_t kid = 0;
+      while (kid < keys.size() && std::memcmp(&keys[kid], &tk, sizeof(tk)) != 0) ++kid;
+      if (kid == keys.size()) keys.push_back(tk);
+      p.tail_kid = kid;
+      tail_levels |= 1u << (p.k - 2);
+    }
+    if (tail_levels) {
+      uint64_t hs = 1024;
+      while (hs < 2 * cap) hs <<= 1;
+      if (ws->hsize != hs) {
+        if ((rc = ws_alloc(ws, (void**)&ws->hkeys, hs * 8))) return rc;
+        if ((rc = ws_alloc(ws, (void**)&ws->hA, hs * 8))) return rc;
+        if ((rc = ws_alloc(ws, (void**)&ws->hAD, hs * 8))) return rc;
+        if ((rc = ws_alloc(ws, (void**)&ws->hnew, hs * 4))) return rc;
+        ws->hsize = hs;
+      }
+      if (ws->tkeys_cap < keys.size()) {
+        if ((rc = ws_alloc(ws, (void**)&ws->tkeys, keys.size() * sizeof(TailKey)))) return rc;
+        ws->tkeys_cap = uint32_t(keys.size());
+      }
+      MG_CK(cudaMemcpyAsync(ws->tkeys, keys.data(), keys.size() * sizeof(TailKey),
+                            cudaMemcpyHostToDevice, st));
+      MG_CK(cudaMemcpyAsync(ws->plans, plans.data(), nq * sizeof(PlanDev), cudaMemcpyHostToDevice,
+                            st));
+      MG_CK(cudaMemsetAsync(ws->hkeys, 0xFF, ws->hsize * 8, st));
+      a.hkeys = ws->hkeys;
+      a.hA = ws->hA;
+      a.hAD = ws->hAD;
+      a.hnew = ws->hnew;
+      a.hmask = ws->hsize - 1;
+      a.tkeys = ws->tkeys;
+    }
   }
-  auto launch_work_scan = [&](int l, bool probe) -> int {
-    a.probe = probe ? 1u : 0u;
+  uint64_t memo_fill = 0;  // slots used in the memo table
+  auto launch_work_scan = [&](int l) -> int {
+    a.tail_on = (tail_levels >> l) & 1u;
+    if (a.tail_on) {
+      // Keep the memo table at most half full: clear it when this chunk's
+      // rows could push it past that.
+      if (memo_fill + R[l] > ws->hsize / 2) {
+        MG_CK(cudaMemsetAsync(ws->hkeys, 0xFF, ws->hsize * 8, st));
+        MG_CK(cudaMemsetAsync(ws->ctr + C_HNEW, 0, 8, st));
+        memo_fill = 0;
+      }
+      k_tail_collect<<<grid_for(R[l], 256, sms * 16), 256, 0, st>>>(a);
+      k_tail_compute<<<grid_for(uint64_t(R[l]) * 32, 256, sms * 16), 256, 0, st>>>(a, memo_fill);
+      res->launches += 2;
+    }
     k_work<<<grid_for(R[l], 256, sms * 16), 256, 0, st>>>(a);
     const uint32_t nb = (R[l] + SCAN_TILE - 1) / SCAN_TILE;
     k_scan_reduce<<<nb, 256, 0, st>>>(ws->work[l], R[l], ws->bsum);
@@ -889,10 +1050,11 @@ static int run_levels(DevGraph* dg, const std::vector<PlanDev>& plans, bool coun
     k_scan_apply<<<nb, 256, 0, st>>>(ws->work[l], R[l], ws->bsum, ws->woff[l]);
     res->launches += 4;
     MG_CK(cudaMemcpyAsync(&ws->h_ctr[0], ws->woff[l] + R[l], 8, cudaMemcpyDeviceToHost, st));
-    if (probe)
-      MG_CK(cudaMemcpyAsync(&ws->h_ctr[C_PROBE_BALG], ws->ctr + C_PROBE_BALG, 16,
-                            cudaMemcpyDeviceToHost, st));
+    if (a.tail_on)
+      MG_CK(cudaMemcpyAsync(&ws->h_ctr[C_HNEW], ws->ctr + C_HNEW, 8, cudaMemcpyDeviceToHost, st));
     MG_CK(cudaStreamSynchronize(st));
+    if (a.tail_on) memo_fill = ws->h_ctr[C_HNEW];
+    a.tail_on = 0;
     return MG_OK;
   };
   auto tab = [&](int l) {
@@ -910,53 +1072,20 @@ static int run_levels(DevGraph* dg, const std::vector<PlanDev>& plans, bool coun
       a.woff = ws->woff[lvl];
       a.dstart = ws->dstart[lvl];
       a.dci = ws->dci[lvl];
-      a.tailA = nullptr;
-      a.tailAD = nullptr;
-      const bool at_tail = tail_possible && lvl == tail_lvl;
-      if (at_tail && !tail_ready) {
-        // Probe: plain work pass whose byte charges are kept aside.
-        MG_CK(cudaMemsetAsync(ws->ctr + C_PROBE_BALG, 0, 16, st));
-        if ((rc = launch_work_scan(lvl, true))) return rc;
-        tail_T += ws->h_ctr[0];
-        if (tail_forced || 2 * tail_T >= tail_cost) {
-          if (!ws->tailA) {
-            if ((rc = ws_alloc(ws, (void**)&ws->tailA, uint64_t(dg->g.n) * 8))) return rc;
-            if ((rc = ws_alloc(ws, (void**)&ws->tailAD, uint64_t(dg->g.n) * 8))) return rc;
-          }
-          const PlanDev& P = plans[0];
-          const uint32_t lp = P.label[P.tail_p];
-          const uint64_t nbk = dg->h_bucket_off[lp + 1] - dg->h_bucket_off[lp];
-          k_tail_aggregate<<<grid_for(nbk * 32, 256, sms * 16), 256, 0, st>>>(
-              dg->g, lp, P.tail_da, P.label[tail_lvl], P.tail_db, P.label[tail_lvl + 1],
-              ws->tailA, ws->tailAD);
-          res->launches++;
-          tail_ready = true;
-        } else {
-          extra_balg += ws->h_ctr[C_PROBE_BALG];
-          extra_balgc += ws->h_ctr[C_PROBE_BALGC];
-          T[lvl] = ws->h_ctr[0];
-        }
-      }
-      if (at_tail && tail_ready) {
-        // Every row is counted in closed form; nothing is expanded.
-        a.tailA = ws->tailA;
-        a.tailAD = ws->tailAD;
-        a.probe = 0;
-        k_work<<<grid_for(R[lvl], 256, sms * 16), 256, 0, st>>>(a);
-        res->launches++;
-        a.tailA = nullptr;
-        a.tailAD = nullptr;
-        T[lvl] = 0;
-      } else if (!at_tail) {
-        if ((rc = launch_work_scan(lvl, false))) return rc;
-        T[lvl] = ws->h_ctr[0];
-      }
+      if ((rc = launch_work_scan(lvl))) return rc;
+      T[lvl] = ws->h_ctr[0];
       cur[lvl] = 0;
       need_work = false;
     }
     if (cur[lvl] < T[lvl]) {
       const uint64_t t0 = cur[lvl];
       const uint64_t t1 = writes[lvl] ? std::min(T[lvl], t0 + cap) : T[lvl];
+      elements += t1 - t0;
+      if (o.max_elements && elements > o.max_elements) {
+        cudaStreamSynchronize(st);
+        return set_error(MG_E_LIMIT, "work budget of %llu candidate elements exceeded",
+                         (unsigned long long)o.max_elements);
+      }
       a.tile_row = ws->tile_row;
       a.level = uint32_t(lvl);
       a.R = R[lvl];
@@ -982,6 +1111,7 @@ static int run_levels(DevGraph* dg, const std::vector<PlanDev>& plans, bool coun
         a.t1 = s1;
         k_tile_rows<<<grid_for(uint64_t(ntiles) + 1, 256, sms * 16), 256, 0, st>>>(
             ws->woff[lvl], R[lvl], s0, s1, ntiles, ws->tile_row);
+        MG_CK(cudaMemsetAsync(ws->ctr + C_TILE, 0, 8, st));
         k_expand<<<grid_for(s1 - s0, EXPAND_BLOCK, sms * 8), EXPAND_BLOCK, 0, st>>>(a);
         res->launches += 2;
       }
@@ -1013,8 +1143,9 @@ static int run_levels(DevGraph* dg, const std::vector<PlanDev>& plans, bool coun
   float ms = 0;
   MG_CK(cudaEventElapsedTime(&ms, ws->ev0, ws->ev1));
   res->ms = ms;
-  res->balg = ws->h_ctr[C_BALG] + extra_balg;
-  res->balgc = ws->h_ctr[C_BALGC] + extra_balgc;
+  res->elements = elements;
+  res->balg = ws->h_ctr[C_BALG];
+  res->balgc = ws->h_ctr[C_BALGC];
   res->emitted = ws->h_ctr[C_EMIT];
   for (int i = 0; i < MAXK + 2 && C_SURV + i < C_NUM; ++i) res->surv[i] = ws->h_ctr[C_SURV + i];
   if (ws->h_ctr[C_ERR] & ERR_OVERFLOW) return set_error(MG_E_CUDA, "device table overflow");
@@ -1114,6 +1245,7 @@ static void fill_stats(mg_stats* st, const PlanDev& P, const RunResult& res, uin
   st->device_ms = res.ms;
   st->launches = res.launches;
   st->chunks = res.chunks;
+  st->elements = res.elements;
 }
 
 static int prepare(DevGraph* dg, const mg_csr_view* q, const mg_opts& o, PlanDev* P) {
@@ -1197,6 +1329,7 @@ int subiso_batch(DevGraph* dg, const mg_csr_view* const* qs, uint32_t nq, const 
     st->device_ms = res.ms;
     st->launches = res.launches;
     st->chunks = res.chunks;
+    st->elements = res.elements;
   }
   return MG_OK;
 }
@@ -1575,6 +1708,7 @@ int noalloc_count(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint6
         a.t1 = s1;
         k_tile_rows<<<grid_for(uint64_t(ntiles) + 1, 256, sms * 16), 256, 0, st>>>(
             L.woff[lvl], R[lvl], s0, s1, ntiles, L.tile_row);
+        MG_CK(cudaMemsetAsync(L.ctr + C_TILE, 0, 8, st));
         k_expand<<<grid_for(s1 - s0, EXPAND_BLOCK, sms * 8), EXPAND_BLOCK, 0, st>>>(a);
       }
       MG_CK(cudaGetLastError());

@@ -33,16 +33,16 @@ ORDERS = {"reference": L.MG_ORDER_REFERENCE, "heuristic": L.MG_ORDER_REFERENCE,
 
 def make_opts(order="reference", filters=L.MG_FILTER_ALL, chunk_rows=0, given_order=None,
               model=None, root_range=None, mem_budget_bytes=0, persistent=0,
-              block=0, merge_min=0, no_tail=0):
+              grab=0, no_tail=0, max_elements=0):
     o = L.default_opts()
     o.no_tail = no_tail
+    o.max_elements = max_elements
     o.order = ORDERS[order] if isinstance(order, str) else int(order)
     o.filters = filters
     o.chunk_rows = chunk_rows
     o.mem_budget_bytes = mem_budget_bytes
     o.persistent = persistent
-    o.block = block
-    o.merge_min = merge_min
+    o.grab = grab
     keep = None
     if given_order is not None:
         keep = np.ascontiguousarray(np.asarray(given_order, dtype=np.uint32))
@@ -59,7 +59,8 @@ def stats_dict(st: L.Stats) -> dict:
     k = st.k
     return {"k": k, "order": list(st.order[:k]), "level_rows": list(st.level_rows[:k + 1]),
             "balg_bytes": st.balg_bytes, "balg_count_bytes": st.balg_count_bytes,
-            "device_ms": st.device_ms, "launches": st.launches, "chunks": st.chunks}
+            "device_ms": st.device_ms, "launches": st.launches, "chunks": st.chunks,
+            "elements": st.elements}
 
 
 def plan_order(q: CSRGraph, order="reference", graph: "DeviceGraph | None" = None,

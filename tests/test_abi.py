@@ -79,3 +79,13 @@ def test_shard_roots_partition():
             assert parts[0][0] == 0 and parts[-1][1] == n
             for (a, b), (c, d) in zip(parts, parts[1:]):
                 assert b == c and a <= b
+
+
+def test_subiso_exec_flags():
+    import subprocess
+    exe = os.path.join(ROOT, "matrixgraph_b200", "subiso_exec")
+    r = subprocess.run([exe, "-g", "x/"], capture_output=True, text=True)
+    assert r.returncode != 0 and "-p" in r.stderr
+    r = subprocess.run([exe, "-p", "/nonexistent/", "-g", "/nonexistent/"], capture_output=True,
+                       text=True)
+    assert r.returncode != 0 and "Error" in r.stderr

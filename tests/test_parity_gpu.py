@@ -226,3 +226,38 @@ def test_tail_closed_form(seed):
             assert st["balg_bytes"] == want["balg"], (k, qe, ql, tail)
             assert st["balg_count_bytes"] == want["balg_count"], (k, qe, ql, tail)
     dg.free()
+
+
+def test_subiso_exec_cli(tmp_path, c1):
+    """The C++ subiso_exec (reference flags) over the C-ABI, exact count and rows."""
+    import subprocess
+    g, q, dg = c1
+    g.Write(str(tmp_path / "g") + "/")
+    q.Write(str(tmp_path / "p") + "/")
+    exe = os.path.join(os.path.dirname(mg.__file__), "subiso_exec")
+    out = tmp_path / "m.txt"
+    r = subprocess.run([exe, "-p", str(tmp_path / "p") + "/", "-g", str(tmp_path / "g") + "/",
+                        "-e", "", "-o", str(out), "-scheduler", "CHBL", "-mode", "emit"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = out.read_text().split()
+    assert int(lines[0]) == dg.count(q)
+    rows = np.array([[int(x) for x in ln.split(",")] for ln in lines[1:]], dtype=np.uint32)
+    assert np.array_equal(rows.reshape(-1, 4), dg.emit(q))
+
+
+def test_tail_memo_batch_and_clearing():
+    """Memoised tail aggregates in batch mode, including memo-table clearing."""
+    g = mg.rmat(13, n_labels=6)
+    dg = mg.DeviceGraph(g)
+    rng = np.random.default_rng(5)
+    qs = []
+    for k, qe in TAIL_QUERIES[:4]:
+        for _ in range(2):
+            qs.append(mg.CSRGraph.query(k, qe, rng.integers(0, 6, k).tolist()))
+    ref = [dg.count(q, no_tail=1) for q in qs]
+    assert [dg.count(q) for q in qs] == ref
+    assert dg.batch_count(qs).tolist() == ref
+    # 4096-row chunks: the memo table (8192 slots) is cleared between chunks
+    assert dg.batch_count(qs, chunk_rows=4096).tolist() == ref
+    dg.free()
