@@ -106,9 +106,10 @@ typedef struct mg_opts {
                                 tail (count mode): 0 or 2 = whenever the plan
                                 ends in one, 1 = never                       */
   uint32_t _reserved;
-  uint64_t max_elements;     /* work budget: candidate elements expanded by
-                                one call; above it the call returns
-                                MG_E_LIMIT (0 = unlimited)                   */
+  uint64_t max_elements;     /* work budget in candidate elements (0 = none):
+                                a single-query call above it returns
+                                MG_E_LIMIT; in a batch it applies per query
+                                and a query above it reports UINT64_MAX      */
 } mg_opts;
 
 /* Per-call statistics (optional out-parameter of the *_ex entry points). */
@@ -248,6 +249,50 @@ int  mg_subiso_batch_count(void* dgraph, const mg_csr_view* const* qs,
 int  mg_subiso_batch_count_ex(void* dgraph, const mg_csr_view* const* qs,
                               uint32_t nq, const mg_opts* opts,
                               uint64_t* counts, mg_stats* st);
+
+/* Batch count with one matching order per query (orders[q*16 + i], query
+ * local ids; NULL = opts->order for all) and, optionally, the surviving
+ * prefixes of every query: level_rows[q*(MG_MAX_QUERY_VERTICES+1) + i] = P_i
+ * (i = 1..k; P_k = count).  These per-prefix counts are what the order model
+ * learns from.  Replaces nq calls of SubIso::Run with a chosen order
+ * (core/task/gpu_task/subiso.cu:236-260).                                  */
+int  mg_subiso_batch_count_orders(void* dgraph, const mg_csr_view* const* qs, uint32_t nq,
+                                  const uint32_t* orders, const mg_opts* opts,
+                                  uint64_t* counts, uint64_t* level_rows, mg_stats* st);
+
+/* ---- learned matching order ---------------------------------------------- *
+ * A message-passing network over the query graph (2 layers, 64 hidden units)
+ * predicts log(1 + P(S)) for connected vertex sets S of a query from the data
+ * graph's label statistics; MG_ORDER_LEARNED picks the order with the least
+ * predicted work.  Orders change work only, never counts.  Training uses
+ * FP32 forward/backward CUDA kernels and Adam; inference uses BF16 weights.
+ * Files reuse the reference's matrix container (<dir>/meta.yaml with x, y and
+ * <dir>/embedding.bin, core/data_structures/matrix.cu:12-35).  The
+ * reference's learned component, MatrixFilter (core/task/cpu_task/
+ * cpu_subiso.cu:237-277), is a lossy candidate filter; this one is an order. */
+int  mg_order_model_create(int device, uint64_t seed, void** model);
+int  mg_order_model_load(const char* dir, int device, void** model);
+int  mg_order_model_save(void* model, const char* dir);
+void mg_order_model_free(void* model);
+int  mg_order_model_num_params(void);
+int  mg_order_model_get_params(void* model, float* out);
+int  mg_order_model_set_params(void* model, const float* params);
+/* Samples are (query index into qs, vertex-set mask over query local ids,
+ * target log(1 + P)).  The loss is the mean squared error over the samples. */
+int  mg_order_model_train(void* model, void* dgraph, const mg_csr_view* const* qs, uint32_t nq,
+                          const uint32_t* s_query, const uint32_t* s_mask, const float* s_target,
+                          uint32_t ns, uint32_t epochs, uint32_t batch, float lr, uint64_t seed,
+                          float* final_loss);
+int  mg_order_model_grad(void* model, void* dgraph, const mg_csr_view* const* qs, uint32_t nq,
+                         const uint32_t* s_query, const uint32_t* s_mask, const float* s_target,
+                         uint32_t ns, float* grad_out, float* loss_out, float* pred_out);
+int  mg_order_model_predict(void* model, void* dgraph, const mg_csr_view* const* qs, uint32_t nq,
+                            const uint32_t* s_query, const uint32_t* s_mask, uint32_t ns,
+                            float* out);
+/* Network inputs of one query: x[16][8] (feature 5 = degree inside S is
+ * computed per sample and left 0), e[16][16], adjacency masks adj[16].      */
+int  mg_order_model_features(void* dgraph, const mg_csr_view* q, float* x, float* e,
+                             uint32_t* adj);
 
 /* Exact count that allocates nothing.  No counterpart in the reference.
  *

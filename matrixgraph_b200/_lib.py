@@ -131,6 +131,27 @@ _SIGS = {
     "mg_subiso_batch_count_ex": (C.c_int, [_VP, C.POINTER(_PV), C.c_uint32, C.POINTER(Opts),
                                            _PU64, C.POINTER(Stats)]),
     "mg_subiso_count_noalloc": (C.c_int, [_VP, _PV, C.POINTER(Opts), _PU64]),
+    "mg_subiso_batch_count_orders": (C.c_int, [_VP, C.POINTER(_PV), C.c_uint32, P32,
+                                               C.POINTER(Opts), _PU64, _PU64,
+                                               C.POINTER(Stats)]),
+    "mg_order_model_create": (C.c_int, [C.c_int, C.c_uint64, _PVP]),
+    "mg_order_model_load": (C.c_int, [C.c_char_p, C.c_int, _PVP]),
+    "mg_order_model_save": (C.c_int, [_VP, C.c_char_p]),
+    "mg_order_model_free": (None, [_VP]),
+    "mg_order_model_num_params": (C.c_int, []),
+    "mg_order_model_get_params": (C.c_int, [_VP, C.POINTER(C.c_float)]),
+    "mg_order_model_set_params": (C.c_int, [_VP, C.POINTER(C.c_float)]),
+    "mg_order_model_train": (C.c_int, [_VP, _VP, C.POINTER(_PV), C.c_uint32, P32, P32,
+                                       C.POINTER(C.c_float), C.c_uint32, C.c_uint32,
+                                       C.c_uint32, C.c_float, C.c_uint64,
+                                       C.POINTER(C.c_float)]),
+    "mg_order_model_grad": (C.c_int, [_VP, _VP, C.POINTER(_PV), C.c_uint32, P32, P32,
+                                      C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_float),
+                                      C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "mg_order_model_predict": (C.c_int, [_VP, _VP, C.POINTER(_PV), C.c_uint32, P32, P32,
+                                         C.c_uint32, C.POINTER(C.c_float)]),
+    "mg_order_model_features": (C.c_int, [_VP, _PV, C.POINTER(C.c_float),
+                                          C.POINTER(C.c_float), P32]),
 }
 
 EXPORTED = tuple(_SIGS)

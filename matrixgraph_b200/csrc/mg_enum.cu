@@ -64,6 +64,8 @@ struct Workspace {
   unsigned long long* ctr = nullptr;     // device counters
   unsigned long long* h_ctr = nullptr;   // pinned mirror
   unsigned long long* counts = nullptr;  // per query
+  unsigned long long* lvl_rows = nullptr;  // per query, MAXK + 1 prefix lengths
+  unsigned long long* q_elems = nullptr;   // per query, elements scheduled
   uint32_t counts_cap = 0;
   PlanDev* plans = nullptr;
   uint32_t plans_cap = 0;
@@ -132,6 +134,8 @@ static int ensure_ws(DevGraph* dg, uint64_t cap, int levels, uint32_t nq) {
   if (ws->counts_cap < nq) {
     int rc;
     if ((rc = ws_alloc(ws, (void**)&ws->counts, uint64_t(nq) * 8))) return rc;
+    if ((rc = ws_alloc(ws, (void**)&ws->lvl_rows, uint64_t(nq) * (MAXK + 1) * 8))) return rc;
+    if ((rc = ws_alloc(ws, (void**)&ws->q_elems, uint64_t(nq) * 8))) return rc;
     if ((rc = ws_alloc(ws, (void**)&ws->plans, uint64_t(nq) * sizeof(PlanDev)))) return rc;
     ws->counts_cap = ws->plans_cap = nq;
   }
@@ -173,6 +177,9 @@ struct StepArgs {
   uint64_t out_cap;
   unsigned long long* ctr;
   unsigned long long* counts;
+  unsigned long long* lvl_rows;  // per query: surviving prefixes of length 0..MAXK
+  unsigned long long* q_elems;   // per query: candidate elements scheduled so far
+  unsigned long long q_budget;   // per-query element budget (0: none)
   uint32_t count_mode;
   uint32_t filters;
   uint32_t stats;
@@ -278,6 +285,34 @@ __device__ __forceinline__ uint64_t memo_find(const StepArgs& a, uint64_t key) {
 
 __device__ __forceinline__ bool tail_row(const StepArgs& a, const PlanDev& P) {
   return a.tail_on && P.tail2 && a.level + 2 == P.k;
+}
+
+// Adds a thread's accumulated match count and prefix survivors of query q:
+// s1 prefixes of length i+1 and sk prefixes of length k (closed-form counts).
+__device__ __forceinline__ void acc_flush(const StepArgs& a, uint32_t q, uint32_t i,
+                                          unsigned long long cnt, unsigned long long s1,
+                                          unsigned long long sk) {
+  if (cnt) atomicAdd(&a.counts[q], cnt);
+  unsigned long long* L = a.lvl_rows + uint64_t(q) * (MAXK + 1);
+  if (s1) atomicAdd(&L[i + 1], s1);
+  if (sk) atomicAdd(&L[a.plans[q].k], sk);
+}
+
+// Flush of a warp's accumulators: one atomic per value when every lane holds
+// the same query, else one per lane.
+__device__ __forceinline__ void acc_flush_warp(const StepArgs& a, uint32_t q, uint32_t i,
+                                               unsigned long long& cnt,
+                                               unsigned long long& s1,
+                                               unsigned long long& sk, bool force) {
+  const bool uniform = __all_sync(FULL, q == __shfl_sync(FULL, q, 0));
+  if (uniform) {
+    const unsigned long long c = warp_sum(cnt), x = warp_sum(s1), y = warp_sum(sk);
+    if ((threadIdx.x & 31) == 0) acc_flush(a, q, i, c, x, y);
+    cnt = s1 = sk = 0;
+  } else if (force) {
+    acc_flush(a, q, i, cnt, s1, sk);
+    cnt = s1 = sk = 0;
+  }
 }
 
 // Inserts (tail key, m_p) of every tail row; new slots are listed in hnew.
@@ -417,8 +452,9 @@ __global__ void __launch_bounds__(256) k_work(StepArgs a) {
       ch = 8ull + 4ull * (e - s) + 8ull * pre + 4ull * dsum;
       chc = 8ull + 4ull * (e - s) + 8ull * pre;
       if (q != tq) {
-        if (tcnt) atomicAdd(&a.counts[tq], tcnt);
-        tcnt = 0;
+        acc_flush(a, tq, i, tcnt, tpre, 0);  // P_{k-1} at i+1, P_k via counts below
+        if (tcnt) atomicAdd(&a.lvl_rows[uint64_t(tq) * (MAXK + 1) + i + 2], tcnt);
+        tcnt = tpre = 0;
         tq = q;
       }
       tcnt += cnt;
@@ -458,6 +494,12 @@ __global__ void __launch_bounds__(256) k_work(StepArgs a) {
       }
       chc = (i + 1 == P.k && P.last_o1) ? 8ull : ch;
     }
+    if (a.q_budget && best) {
+      // Per-query budget: a query whose scheduled elements pass the budget
+      // stops expanding (its count is reported as unknown).
+      const unsigned long long before = atomicAdd(&a.q_elems[q], (unsigned long long)best);
+      if (before + best > a.q_budget) best = 0;
+    }
     a.work[r] = best;
     a.dstart[r] = bs;
     a.dci[r] = bci;
@@ -471,19 +513,15 @@ __global__ void __launch_bounds__(256) k_work(StepArgs a) {
     atomicAdd(&a.ctr[C_BALGC], balc);
   }
   if (a.tail_on) {
-    if (a.stats) {  // single query: P_{k-1} and P_k of the tail rows
-      unsigned long long sp = warp_sum(tpre), sc = warp_sum(tcnt);
-      if ((threadIdx.x & 31) == 0) {
-        if (sp) atomicAdd(&a.ctr[C_SURV + i + 1], sp);
-        if (sc) atomicAdd(&a.ctr[C_SURV + i + 2], sc);
-      }
+    const bool uniform = __all_sync(FULL, tq == __shfl_sync(FULL, tq, 0));
+    unsigned long long c = tcnt, p = tpre;
+    if (uniform) {
+      c = warp_sum(tcnt);
+      p = warp_sum(tpre);
     }
-    const uint32_t same = __match_any_sync(FULL, tq);
-    if (same == FULL) {
-      const unsigned long long sc = warp_sum(tcnt);
-      if ((threadIdx.x & 31) == 0 && sc) atomicAdd(&a.counts[tq], sc);
-    } else if (tcnt) {
-      atomicAdd(&a.counts[tq], tcnt);
+    if (!uniform || (threadIdx.x & 31) == 0) {
+      acc_flush(a, tq, i, c, p, 0);
+      if (c) atomicAdd(&a.lvl_rows[uint64_t(tq) * (MAXK + 1) + i + 2], c);
     }
   }
 }
@@ -597,7 +635,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t span = a.t1 - a.t0;
   const uint64_t ntiles = (span + EXPAND_BLOCK - 1) / EXPAND_BLOCK;
-  unsigned long long cnt = 0, bal = 0, balc = 0, surv1 = 0, survk = 0;
+  unsigned long long cnt = 0, bal = 0, balc = 0, s1 = 0, sk = 0;
   uint32_t cnt_q = 0;
   // Device work queue: each block takes `grab` consecutive tiles at a time,
   // so a block walks contiguous element ranges (same rows, same query) and a
@@ -660,16 +698,14 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
       if (ok && !fin && a.filters && !(i + 2 == P.k && P.last_o1))
         ok = pass_filters(g, P, i, x, a.filters);
       if (ok) {
-        surv1 += 1;
+        if (q != cnt_q) {
+          acc_flush(a, cnt_q, i, cnt, s1, sk);
+          cnt = s1 = sk = 0;
+          cnt_q = q;
+        }
+        s1 += 1;
         if (fin) {
-          if (a.count_mode) {
-            if (q != cnt_q) {
-              if (cnt) atomicAdd(&a.counts[cnt_q], cnt);
-              cnt = 0;
-              cnt_q = q;
-            }
-            cnt += 1;
-          }
+          if (a.count_mode) cnt += 1;
         } else if (fused) {
           const uint32_t kl = P.k - 1;
           const uint32_t cs = P.cons[kl][0];
@@ -689,12 +725,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
               c1 -= contains(g.adj[dir], s, en, mj) ? 1ull : 0ull;
             }
           }
-          survk += c1;
-          if (q != cnt_q) {
-            if (cnt) atomicAdd(&a.counts[cnt_q], cnt);
-            cnt = 0;
-            cnt_q = q;
-          }
+          sk += c1;
           cnt += c1;
         }
       }
@@ -751,33 +782,14 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
     __syncthreads();  // s_wcnt / s_wbase are reused by the next tile
   }
   // Once per grab: fold the per-thread counts of a warp that holds one query.
-  if (__all_sync(FULL, cnt_q == __shfl_sync(FULL, cnt_q, 0))) {
-    const unsigned long long sc = warp_sum(cnt);
-    if (lane == 0 && sc) atomicAdd(&a.counts[cnt_q], sc);
-    cnt = 0;
-  }
+  acc_flush_warp(a, cnt_q, i, cnt, s1, sk, false);
   }  // grab loop
-  // Flush per-thread counts: warp-reduce when the whole warp holds one query.
-  const uint32_t same = __match_any_sync(FULL, cnt_q);
-  if (same == FULL) {
-    unsigned long long s = warp_sum(cnt);
-    if (lane == 0 && s) atomicAdd(&a.counts[cnt_q], s);
-  } else if (cnt) {
-    atomicAdd(&a.counts[cnt_q], cnt);
-  }
+  acc_flush_warp(a, cnt_q, i, cnt, s1, sk, true);
   bal = warp_sum(bal);
   balc = warp_sum(balc);
   if (lane == 0 && (bal | balc)) {
     atomicAdd(&a.ctr[C_BALG], bal);
     atomicAdd(&a.ctr[C_BALGC], balc);
-  }
-  if (a.stats) {
-    surv1 = warp_sum(surv1);
-    survk = warp_sum(survk);
-    if (lane == 0) {
-      if (surv1) atomicAdd(&a.ctr[C_SURV + i + 1], surv1);
-      if (survk) atomicAdd(&a.ctr[C_SURV + a.plans[0].k], survk);
-    }
   }
 }
 
@@ -919,7 +931,7 @@ static inline unsigned grid_for(uint64_t items, unsigned block, unsigned cap) {
 
 static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
                       const EmitBuf* emit, const mg_opts& o, uint64_t* counts_out,
-                      RunResult* res) {
+                      RunResult* res, uint64_t* lvl_rows_out = nullptr) {
   const uint32_t nq = uint32_t(plans.size());
   uint32_t kmax = 1;
   for (auto& p : plans) kmax = std::max(kmax, p.k);
@@ -945,6 +957,8 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
   cudaStream_t st = dg->stream;
   MG_CK(cudaMemcpyAsync(ws->plans, plans.data(), nq * sizeof(PlanDev), cudaMemcpyHostToDevice, st));
   MG_CK(cudaMemsetAsync(ws->counts, 0, nq * 8ull, st));
+  MG_CK(cudaMemsetAsync(ws->lvl_rows, 0, uint64_t(nq) * (MAXK + 1) * 8, st));
+  MG_CK(cudaMemsetAsync(ws->q_elems, 0, uint64_t(nq) * 8, st));
   MG_CK(cudaMemsetAsync(ws->ctr, 0, C_NUM * 8, st));
   MG_CK(cudaEventRecord(ws->ev0, st));
 
@@ -960,6 +974,9 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
   a.plans = ws->plans;
   a.ctr = ws->ctr;
   a.counts = ws->counts;
+  a.lvl_rows = ws->lvl_rows;
+  a.q_elems = ws->q_elems;
+  a.q_budget = nq > 1 ? o.max_elements : 0;  // batch: per-query budget
   a.count_mode = count_mode ? 1u : 0u;
   a.filters = o.filters & MG_FILTER_ALL;
   a.grab = o.grab;
@@ -990,8 +1007,10 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
   // Pendant tails counted in closed form (count mode): tail-key table and
   // memo table of two-hop aggregates, shared by every query of the call.
   uint32_t tail_levels = 0;
+  uint64_t hsize_used = 0, keyspace = 0;
   if (count_mode && o.no_tail != 1) {
     std::vector<TailKey> keys;
+    std::vector<uint64_t> key_lp;  // (kid << 32 | label of m_p): key space per pair
     for (PlanDev& p : plans) {
       if (!p.tail2) continue;
       const TailKey tk{p.tail_da, p.label[p.k - 2], p.tail_db, p.label[p.k - 1]};
@@ -1000,17 +1019,26 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
       if (kid == keys.size()) keys.push_back(tk);
       p.tail_kid = kid;
       tail_levels |= 1u << (p.k - 2);
+      const uint32_t lp = p.label[p.tail_p];
+      const uint64_t kl = (uint64_t(kid) << 32) | lp;
+      if (std::find(key_lp.begin(), key_lp.end(), kl) == key_lp.end()) {
+        key_lp.push_back(kl);
+        keyspace += dg->h_bucket_off[lp + 1] - dg->h_bucket_off[lp];
+      }
     }
     if (tail_levels) {
+      // Table size: twice the distinct keys that can occur (vertices of the
+      // label bucket of m_p per tail signature), at most 4 * cap slots.
       uint64_t hs = 1024;
-      while (hs < 2 * cap) hs <<= 1;
-      if (ws->hsize != hs) {
+      while (hs < 2 * std::min<uint64_t>(keyspace, 2 * cap)) hs <<= 1;
+      if (ws->hsize < hs) {
         if ((rc = ws_alloc(ws, (void**)&ws->hkeys, hs * 8))) return rc;
         if ((rc = ws_alloc(ws, (void**)&ws->hA, hs * 8))) return rc;
         if ((rc = ws_alloc(ws, (void**)&ws->hAD, hs * 8))) return rc;
         if ((rc = ws_alloc(ws, (void**)&ws->hnew, hs * 4))) return rc;
         ws->hsize = hs;
       }
+      hsize_used = hs;
       if (ws->tkeys_cap < keys.size()) {
         if ((rc = ws_alloc(ws, (void**)&ws->tkeys, keys.size() * sizeof(TailKey)))) return rc;
         ws->tkeys_cap = uint32_t(keys.size());
@@ -1019,12 +1047,12 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
                             cudaMemcpyHostToDevice, st));
       MG_CK(cudaMemcpyAsync(ws->plans, plans.data(), nq * sizeof(PlanDev), cudaMemcpyHostToDevice,
                             st));
-      MG_CK(cudaMemsetAsync(ws->hkeys, 0xFF, ws->hsize * 8, st));
+      MG_CK(cudaMemsetAsync(ws->hkeys, 0xFF, hsize_used * 8, st));
       a.hkeys = ws->hkeys;
       a.hA = ws->hA;
       a.hAD = ws->hAD;
       a.hnew = ws->hnew;
-      a.hmask = ws->hsize - 1;
+      a.hmask = hsize_used - 1;
       a.tkeys = ws->tkeys;
     }
   }
@@ -1034,8 +1062,8 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
     if (a.tail_on) {
       // Keep the memo table at most half full: clear it when this chunk's
       // rows could push it past that.
-      if (memo_fill + R[l] > ws->hsize / 2) {
-        MG_CK(cudaMemsetAsync(ws->hkeys, 0xFF, ws->hsize * 8, st));
+      if (memo_fill + std::min<uint64_t>(R[l], keyspace) > hsize_used / 2) {
+        MG_CK(cudaMemsetAsync(ws->hkeys, 0xFF, hsize_used * 8, st));
         MG_CK(cudaMemsetAsync(ws->ctr + C_HNEW, 0, 8, st));
         memo_fill = 0;
       }
@@ -1081,7 +1109,7 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
       const uint64_t t0 = cur[lvl];
       const uint64_t t1 = writes[lvl] ? std::min(T[lvl], t0 + cap) : T[lvl];
       elements += t1 - t0;
-      if (o.max_elements && elements > o.max_elements) {
+      if (nq == 1 && o.max_elements && elements > o.max_elements) {
         cudaStreamSynchronize(st);
         return set_error(MG_E_LIMIT, "work budget of %llu candidate elements exceeded",
                          (unsigned long long)o.max_elements);
@@ -1138,16 +1166,26 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
   MG_CK(cudaEventRecord(ws->ev1, st));
   MG_CK(cudaMemcpyAsync(ws->h_ctr, ws->ctr, C_NUM * 8, cudaMemcpyDeviceToHost, st));
   MG_CK(cudaMemcpyAsync(counts_out, ws->counts, nq * 8ull, cudaMemcpyDeviceToHost, st));
+  if (lvl_rows_out)
+    MG_CK(cudaMemcpyAsync(lvl_rows_out, ws->lvl_rows, uint64_t(nq) * (MAXK + 1) * 8,
+                          cudaMemcpyDeviceToHost, st));
+  MG_CK(cudaMemcpyAsync(res->surv, ws->lvl_rows, (MAXK + 1) * 8, cudaMemcpyDeviceToHost, st));
+  std::vector<unsigned long long> qel;
+  if (a.q_budget) {
+    qel.resize(nq);
+    MG_CK(cudaMemcpyAsync(qel.data(), ws->q_elems, uint64_t(nq) * 8, cudaMemcpyDeviceToHost, st));
+  }
   MG_CK(cudaStreamSynchronize(st));
   MG_CK(cudaGetLastError());
   float ms = 0;
   MG_CK(cudaEventElapsedTime(&ms, ws->ev0, ws->ev1));
   res->ms = ms;
   res->elements = elements;
+  for (uint32_t q = 0; q < qel.size(); ++q)
+    if (qel[q] > a.q_budget) counts_out[q] = ~0ull;  // over budget: unknown
   res->balg = ws->h_ctr[C_BALG];
   res->balgc = ws->h_ctr[C_BALGC];
   res->emitted = ws->h_ctr[C_EMIT];
-  for (int i = 0; i < MAXK + 2 && C_SURV + i < C_NUM; ++i) res->surv[i] = ws->h_ctr[C_SURV + i];
   if (ws->h_ctr[C_ERR] & ERR_OVERFLOW) return set_error(MG_E_CUDA, "device table overflow");
   return MG_OK;
 }
@@ -1312,15 +1350,40 @@ int subiso_emit(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint32_
 }
 
 int subiso_batch(DevGraph* dg, const mg_csr_view* const* qs, uint32_t nq, const mg_opts* opts,
-                 uint64_t* counts, mg_stats* st) {
+                 uint64_t* counts, mg_stats* st, const uint32_t* orders = nullptr,
+                 uint64_t* level_rows = nullptr) {
   const mg_opts o = resolve_opts(opts);
   std::vector<PlanDev> plans(nq);
+  std::vector<uint32_t> learned;
+  if (!orders && o.order == MG_ORDER_LEARNED && o.model) {
+    // One inference launch plans the whole batch.
+    int rc = ensure_full_stats(dg);
+    if (rc) return rc;
+    std::vector<QueryGraph> Q(nq);
+    std::vector<const QueryGraph*> qp(nq);
+    for (uint32_t i = 0; i < nq; ++i) {
+      if ((rc = normalise_query(qs[i], &Q[i])))
+        return set_error(rc, "query %u: %s", i, last_error_cstr());
+      qp[i] = &Q[i];
+    }
+    std::vector<std::array<uint32_t, MAXK>> ord;
+    if ((rc = order_learned_batch(o.model, qp, dg->stats, ord))) return rc;
+    learned.resize(uint64_t(nq) * MAXK);
+    for (uint32_t i = 0; i < nq; ++i)
+      std::memcpy(&learned[uint64_t(i) * MAXK], ord[i].data(), MAXK * 4);
+    orders = learned.data();
+  }
   for (uint32_t i = 0; i < nq; ++i) {
-    int rc = prepare(dg, qs[i], o, &plans[i]);
+    mg_opts oi = o;
+    if (orders) {
+      oi.order = MG_ORDER_GIVEN;
+      oi.given_order = orders + uint64_t(i) * MAXK;
+    }
+    int rc = prepare(dg, qs[i], oi, &plans[i]);
     if (rc) return set_error(rc, "query %u: %s", i, last_error_cstr());
   }
   RunResult res;
-  int rc = run_levels(dg, plans, true, nullptr, o, counts, &res);
+  int rc = run_levels(dg, plans, true, nullptr, o, counts, &res, level_rows);
   if (rc) return rc;
   if (st) {
     std::memset(st, 0, sizeof(*st));
@@ -1428,6 +1491,18 @@ int mg_subiso_batch_count(void* dgraph, const mg_csr_view* const* qs, uint32_t n
   return mg_subiso_batch_count_ex(dgraph, qs, nq, opts, counts, nullptr);
 }
 
+int mg_subiso_batch_count_orders(void* dgraph, const mg_csr_view* const* qs, uint32_t nq,
+                                 const uint32_t* orders, const mg_opts* opts, uint64_t* counts,
+                                 uint64_t* level_rows, mg_stats* st) {
+  MG_ENTRY(dgraph);
+  if (!qs || !counts || nq == 0) return mg::set_error(MG_E_ARG, "null argument or empty batch");
+  try {
+    return mg::subiso_batch(dg, qs, nq, opts, counts, st, orders, level_rows);
+  } catch (const std::bad_alloc&) {
+    return mg::set_error(MG_E_OOM, "host allocation failed");
+  }
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
@@ -1472,6 +1547,7 @@ int noalloc_scratch(int device, unsigned char** out) {
 struct NoallocLayout {
   unsigned long long* ctr;
   unsigned long long* counts;
+  unsigned long long* lvl_rows;
   PlanDev* plan;
   uint64_t* bsum;
   uint32_t* tile_row;
@@ -1495,6 +1571,7 @@ uint64_t noalloc_carve(unsigned char* base, uint64_t cap, uint32_t k, NoallocLay
   };
   L->ctr = reinterpret_cast<unsigned long long*>(take(C_NUM * 8));
   L->counts = reinterpret_cast<unsigned long long*>(take(8));
+  L->lvl_rows = reinterpret_cast<unsigned long long*>(take((MAXK + 1) * 8));
   L->plan = reinterpret_cast<PlanDev*>(take(sizeof(PlanDev)));
   L->bsum = reinterpret_cast<uint64_t*>(take((cap / SCAN_TILE + 2) * 8));
   L->tile_row = reinterpret_cast<uint32_t*>(take((kNoallocSegment / EXPAND_BLOCK + 2) * 4));
@@ -1643,6 +1720,7 @@ int noalloc_count(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint6
   // The array keeps the previous call's contents: counters start at zero.
   MG_CK(cudaMemcpyAsync(L.plan, &P, sizeof(PlanDev), cudaMemcpyHostToDevice, st));
   MG_CK(cudaMemsetAsync(L.counts, 0, 8, st));
+  MG_CK(cudaMemsetAsync(L.lvl_rows, 0, (MAXK + 1) * 8, st));
   MG_CK(cudaMemsetAsync(L.ctr, 0, C_NUM * 8, st));
 
   StepArgs a;
@@ -1651,6 +1729,7 @@ int noalloc_count(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint6
   a.plans = L.plan;
   a.ctr = L.ctr;
   a.counts = L.counts;
+  a.lvl_rows = L.lvl_rows;
   a.count_mode = 1;
   a.filters = o.filters & MG_FILTER_ALL;
   a.nq = 1;

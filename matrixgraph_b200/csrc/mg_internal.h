@@ -2,6 +2,7 @@
 // libmg_subiso.so.  Nothing here crosses the C-ABI.
 #pragma once
 
+#include <array>
 #include <cstdint>
 #include <cstdio>
 #include <cstdarg>
@@ -103,5 +104,8 @@ bool order_is_permutation(const uint32_t* order, uint32_t k);
 // Learned order model (mg_order_model.cu).
 int order_learned(void* model, const QueryGraph& q, const GraphStats& gs,
                   uint32_t* order);
+int order_learned_batch(void* model, const std::vector<const QueryGraph*>& qs,
+                        const GraphStats& gs,
+                        std::vector<std::array<uint32_t, MG_MAX_QUERY_VERTICES>>& orders);
 
 }  // namespace mg

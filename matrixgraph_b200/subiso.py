@@ -123,6 +123,25 @@ class DeviceGraph:
                                                C.byref(st)))
         return (counts, stats_dict(st)) if stats else counts
 
+    def batch_count_orders(self, qs: Sequence[CSRGraph], orders, **kw):
+        """Counts and per-prefix survivors P_i of each query under its own order.
+
+        Returns (counts[nq], level_rows[nq, 17], stats)."""
+        o, keep = make_opts(**kw)
+        nq = len(qs)
+        arr = (C.POINTER(L.CsrView) * nq)(*[C.pointer(q.view) for q in qs])
+        ords = np.zeros((nq, L.MG_MAX_QUERY_VERTICES), dtype=np.uint32)
+        for i, od in enumerate(orders):
+            ords[i, :len(od)] = od
+        counts = np.zeros(nq, dtype=np.uint64)
+        rows = np.zeros((nq, L.MG_MAX_QUERY_VERTICES + 1), dtype=np.uint64)
+        st = L.Stats()
+        L.check(L.lib.mg_subiso_batch_count_orders(
+            self.handle, arr, nq, ords.ctypes.data_as(L.P32), C.byref(o),
+            counts.ctypes.data_as(C.POINTER(C.c_uint64)),
+            rows.ctypes.data_as(C.POINTER(C.c_uint64)), C.byref(st)))
+        return counts, rows, stats_dict(st)
+
     def plan_order(self, q: CSRGraph, order="reference", **kw) -> list[int]:
         return plan_order(q, order=order, graph=self, **kw)
 

@@ -14,6 +14,17 @@
   seeds, sizes and counts are committed in ``data/batch_seeds.json``.
 
     python -m matrixgraph_b200.workloads select-batch OUT.json
+    python -m matrixgraph_b200.workloads train-order OUTDIR [N]
+    python -m matrixgraph_b200.workloads eval-order MODEL_DIR/ OUT.json [N]
+    python -m matrixgraph_b200.workloads eval-batch MODEL_DIR/ OUT.json
+
+Learned order: training queries are random connected queries with k uniform
+in 6..10 (seeds from 100000) on the scale-20 graph, kept when the reference
+order needs at most TRAIN_BUDGET elements; the enumerator records P_i for the
+reference order and 8 random connected orders of each (per-query budget).
+Held-out queries use seeds from 200000 on the scale-22 graph.  Both
+selections stop after a fixed time; the kept seeds are committed with the
+model (data/order_train_record.json, data/order_eval.json).
 """
 from __future__ import annotations
 
@@ -84,7 +95,200 @@ def select_batch(dg: DeviceGraph, g, n: int = BATCH_SIZE, budget: int = BATCH_BU
             "counts": counts, "elements": elements, "dropped": dropped}
 
 
+# ---- learned order: training and held-out queries ---------------------------
+TRAIN_SCALE = 20
+TRAIN_FIRST_SEED = 100000
+EVAL_FIRST_SEED = 200000
+TRAIN_BUDGET = 1 << 26
+EVAL_BUDGET = 1 << 27
+MODEL_DIR = os.path.join(HERE, "data", "order_model") + "/"
+
+
+def learned_k(seed: int) -> int:
+    """Query size of a learned-order seed: uniform over 6..10."""
+    return int(np.random.default_rng(seed).integers(6, 11))
+
+
+def learned_query(g, seed: int):
+    return query_random(g, learned_k(seed), 0.3, seed)
+
+
+def select_queries(dg, g, make, first_seed, n, budget, max_candidates, log=None,
+                   max_seconds=None):
+    """First n seeds whose reference-order count needs at most `budget`
+    candidate elements (deterministic: element counts are exact); stops early
+    after max_candidates seeds or max_seconds."""
+    import time
+    t0 = time.time()
+    kept, dropped, s = [], 0, first_seed
+    while len(kept) < n and s - first_seed < max_candidates:
+        if max_seconds and time.time() - t0 > max_seconds:
+            break
+        q = make(g, s)
+        try:
+            c, st = dg.count(q, stats=True, max_elements=budget)
+            kept.append({"seed": s, "k": q.n, "count": int(c), "elements": int(st["elements"]),
+                         "ms": st["device_ms"]})
+        except L.MGError as e:
+            if e.code != L.MG_E_LIMIT:
+                raise
+            dropped += 1
+        s += 1
+        if log and (s - first_seed) % 4000 == 0:
+            log(f"seed {s}: kept {len(kept)} dropped {dropped}")
+    return kept, dropped
+
+
+def train_order(outdir: str, n_train: int = 4000, n_random: int = 8, epochs: int = 60,
+                log=print, select_seconds: float = 200.0):
+    import time
+    from .order_model import OrderModel, record_prefix_counts
+    t0 = time.time()
+    g = rmat_graph(TRAIN_SCALE)
+    dg = DeviceGraph(g)
+    kept, dropped = select_queries(dg, g, learned_query, TRAIN_FIRST_SEED, n_train, TRAIN_BUDGET,
+                                   40 * n_train, log, max_seconds=select_seconds)
+    log(f"train queries: kept {len(kept)} dropped {dropped} ({time.time() - t0:.1f}s)")
+    qs = [learned_query(g, r["seed"]) for r in kept]
+    (sq, sm, st), records = record_prefix_counts(dg, qs, n_random, TRAIN_BUDGET, seed=7)
+    censored = sum(1 for r in records if r[2] == 2 ** 64 - 1)
+    log(f"samples {len(sq)} from {len(records)} runs, {censored} over budget "
+        f"({time.time() - t0:.1f}s)")
+    val = (sq % 10) == 9  # 90/10 split by query: validation loss
+    model = OrderModel.create(seed=0)
+    _, l0, _ = model.grad(dg, qs, sq[~val], sm[~val], st[~val])
+    model.train(dg, qs, sq[~val], sm[~val], st[~val], epochs=epochs, batch=512, lr=2e-3, seed=1)
+    _, ltr, _ = model.grad(dg, qs, sq[~val], sm[~val], st[~val])
+    _, lval, _ = model.grad(dg, qs, sq[val], sm[val], st[val])
+    log(f"loss: init {l0:.3f} train {ltr:.3f} validation {lval:.3f} ({time.time() - t0:.1f}s)")
+    os.makedirs(os.path.join(outdir, "order_model"), exist_ok=True)
+    model.save(os.path.join(outdir, "order_model") + "/")
+    rec = {"graph": f"rmat scale {TRAIN_SCALE} (workloads.rmat_graph)", "budget": TRAIN_BUDGET,
+           "first_seed": TRAIN_FIRST_SEED, "seeds": [r["seed"] for r in kept],
+           "k": [r["k"] for r in kept], "dropped": dropped, "runs": len(records),
+           "censored_runs": censored, "samples": int(len(sq)), "epochs": epochs,
+           "loss_init": l0, "loss_train": ltr, "loss_validation": lval,
+           "seconds": time.time() - t0}
+    with open(os.path.join(outdir, "order_train_record.json"), "w") as f:
+        json.dump(rec, f)
+    return rec
+
+
+def eval_order(model_dir: str, out_path: str, n_eval: int = 2000, log=print,
+               select_seconds: float = 150.0):
+    """Held-out queries (k 6..10) on the scale-22 graph: reference vs learned."""
+    import time
+    from .order_model import OrderModel
+    t0 = time.time()
+    g = rmat_graph(22)
+    dg = DeviceGraph(g)
+    model = OrderModel.load(model_dir)
+    kept, dropped = select_queries(dg, g, learned_query, EVAL_FIRST_SEED, n_eval, EVAL_BUDGET,
+                                   12 * n_eval, log, max_seconds=select_seconds)
+    log(f"held-out: kept {len(kept)} dropped {dropped} ({time.time() - t0:.1f}s)")
+    rows = []
+    for r in kept:
+        q = learned_query(g, r["seed"])
+        c_ref, st_ref = dg.count(q, stats=True)
+        t_plan = time.perf_counter()
+        lo = dg.plan_order(q, order="learned", model=model)
+        t_plan = time.perf_counter() - t_plan
+        guard = max(16 * r["elements"], 1 << 24)
+        try:
+            c_l, st_l = dg.count(q, stats=True, given_order=lo, max_elements=guard)
+            ms_l = st_l["device_ms"]
+            assert c_l == c_ref, (r["seed"], c_l, c_ref)
+        except L.MGError as e:
+            if e.code != L.MG_E_LIMIT:
+                raise
+            ms_l, st_l = float("inf"), None
+        try:
+            _, st_s = dg.count(q, stats=True, order="strong", max_elements=guard)
+            ms_s = st_s["device_ms"]
+        except L.MGError as e:
+            if e.code != L.MG_E_LIMIT:
+                raise
+            ms_s = float("inf")
+        rows.append({"seed": r["seed"], "k": q.n, "count": int(c_ref),
+                     "ms_ref": st_ref["device_ms"], "ms_learned": ms_l, "ms_strong": ms_s,
+                     "plan_ms": 1e3 * t_plan, "order_ref": st_ref["order"],
+                     "order_learned": lo, "rows_ref": st_ref["level_rows"],
+                     "rows_learned": st_l["level_rows"] if st_l else None})
+    sp = np.array([x["ms_ref"] / x["ms_learned"] for x in rows])
+    sp_wall = np.array([x["ms_ref"] / (x["ms_learned"] + x["plan_ms"]) for x in rows])
+    best = np.array([min(x["ms_ref"], x["ms_strong"], x["ms_learned"]) for x in rows])
+    regret = np.array([x["ms_learned"] / b for x, b in zip(rows, best)])
+    summary = {"n": len(rows), "dropped": dropped, "budget": EVAL_BUDGET,
+               "median_speedup_device": float(np.median(sp)) if len(sp) else None,
+               "median_speedup_with_planning": float(np.median(sp_wall)) if len(sp) else None,
+               "geomean_speedup_device": float(np.exp(np.mean(np.log(sp)))) if len(sp) else None,
+               "total_ms_ref": float(sum(x["ms_ref"] for x in rows)),
+               "total_ms_learned": float(sum(x["ms_learned"] for x in rows)),
+               "total_ms_strong": float(sum(x["ms_strong"] for x in rows)),
+               "median_regret": float(np.median(regret)) if len(sp) else None,
+               "learned_over_budget": int(sum(1 for x in rows if x["ms_learned"] == float("inf"))),
+               "seconds": time.time() - t0}
+    log(json.dumps(summary))
+    with open(out_path, "w") as f:
+        json.dump({"summary": summary, "rows": rows}, f)
+    return summary
+
+
+def eval_batch(model_dir: str, out_path: str, log=print):
+    """The committed 4,096-query batch: plain per-query heuristic-order form
+    against the batched forms (reference and learned orders)."""
+    import time
+    from .order_model import OrderModel
+    g = rmat_graph(22)
+    dg = DeviceGraph(g)
+    model = OrderModel.load(model_dir)
+    qs, rec = batch_queries(g)
+    res = {"n": len(qs)}
+    for _ in range(2):  # second pass is the measured one (warm)
+        t = time.perf_counter()
+        dev, counts = 0.0, []
+        for q in qs:
+            c, st = dg.count(q, stats=True)
+            dev += st["device_ms"]
+            counts.append(int(c))
+        res["per_query_reference"] = {"wall_s": time.perf_counter() - t, "device_s": dev / 1e3}
+        assert counts == rec["counts"]
+    for order in ("reference", "learned"):
+        for _ in range(2):
+            t = time.perf_counter()
+            c, st = dg.batch_count(qs, stats=True, order=order, model=model)
+            wall = time.perf_counter() - t
+        assert c.tolist() == rec["counts"]
+        res[f"batch_{order}"] = {"wall_s": wall, "device_s": st["device_ms"] / 1e3,
+                                 "launches": st["launches"], "chunks": st["chunks"]}
+    for _ in range(2):
+        t = time.perf_counter()
+        dev = 0.0
+        for q in qs:
+            c, st = dg.count(q, stats=True, order="learned", model=model)
+            dev += st["device_ms"]
+        res["per_query_learned"] = {"wall_s": time.perf_counter() - t, "device_s": dev / 1e3}
+    base = res["per_query_reference"]["wall_s"]
+    res["per_query_reference"]["queries_per_s"] = len(qs) / base
+    for key in ("batch_reference", "batch_learned", "per_query_learned"):
+        res[key]["speedup_vs_per_query_reference"] = base / res[key]["wall_s"]
+        res[key]["queries_per_s"] = len(qs) / res[key]["wall_s"]
+    log(json.dumps(res))
+    with open(out_path, "w") as f:
+        json.dump(res, f)
+    return res
+
+
 def main(argv):
+    if len(argv) >= 2 and argv[0] == "train-order":
+        train_order(argv[1], n_train=int(argv[2]) if len(argv) > 2 else 4000)
+        return 0
+    if len(argv) >= 3 and argv[0] == "eval-order":
+        eval_order(argv[1], argv[2], n_eval=int(argv[3]) if len(argv) > 3 else 2000)
+        return 0
+    if len(argv) >= 3 and argv[0] == "eval-batch":
+        eval_batch(argv[1], argv[2])
+        return 0
     if len(argv) >= 2 and argv[0] == "select-batch":
         g = rmat_graph(22)
         dg = DeviceGraph(g)

@@ -261,3 +261,27 @@ def test_tail_memo_batch_and_clearing():
     # 4096-row chunks: the memo table (8192 slots) is cleared between chunks
     assert dg.batch_count(qs, chunk_rows=4096).tolist() == ref
     dg.free()
+
+
+def test_batch_orders_level_rows_and_budget(c1):
+    """Per-query orders and prefix counts in one batch equal the oracle's; a
+    per-query budget marks only over-budget queries."""
+    g, q, dg = c1
+    rng = np.random.default_rng(11)
+    qs, orders = [], []
+    for i in range(24):
+        x = mg.query_random(g, 3 + i % 5, 0.3, seed=3000 + i)
+        qs.append(x)
+        orders.append(rng.permutation(x.n).tolist())
+    counts, rows, _ = dg.batch_count_orders(qs, orders)
+    for x, od, c, r in zip(qs, orders, counts, rows):
+        want = oracle_count(g, x, order=od)
+        assert c == want["count"]
+        assert r[:x.n + 1].tolist() == want["level_rows"]
+    budget = int(np.median([dg.count(x, stats=True)[1]["elements"] for x in qs]))
+    counts_b, _, _ = dg.batch_count_orders(qs, [mg.plan_order(x) for x in qs],
+                                           max_elements=max(budget, 1))
+    singles = [dg.count(x) for x in qs]
+    for cb, cs_ in zip(counts_b, singles):
+        assert cb == cs_ or cb == 2 ** 64 - 1
+    assert any(cb == 2 ** 64 - 1 for cb in counts_b)
