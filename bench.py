@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--queries", default="",
                    help="comma-separated subset of the query shapes (profiling runs)")
+    p.add_argument("--no-batch", action="store_true",
+                   help="skip the batched-workload measurement")
     return p.parse_args()
 
 
@@ -148,21 +150,6 @@ def dist_setup(args):
     return world, rank, local
 
 
-def first_bucket_sizes(g, qs, dg=None):
-    """Level-0 candidate count of each query (its first vertex's label bucket)."""
-    import numpy as np
-
-    import matrixgraph_b200 as mg
-    lab = g.array("labels")
-    vals, cnts = np.unique(lab, return_counts=True)
-    size = dict(zip(vals.tolist(), cnts.tolist()))
-    out = []
-    for q in qs:
-        order = mg.plan_order(q)
-        out.append(int(size.get(int(q.array("labels")[order[0]]), 0)))
-    return out
-
-
 def cpu_baseline(g, qs, target_s):
     """The oracle (exact CPU port, all host threads) on a bounded sample of roots."""
     import oracle as O
@@ -240,6 +227,49 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def batched_workload(g, dg):
+    """The committed 4,096-query batch on the same resident graph: the plain
+    per-query heuristic-order form against one batched call with learned
+    orders (planning included), wall clock, counts checked per query."""
+    import matrixgraph_b200 as mg
+    from matrixgraph_b200 import workloads as W
+    from matrixgraph_b200.order_model import OrderModel
+    qs, rec = W.batch_queries(g)
+    model = OrderModel.load(W.MODEL_DIR)
+    out = {"workload": f"{len(qs)} random connected queries (k 3-8, p_extra 0.3, random-walk "
+                       "labels; seeds kept when the reference order needs <= 2^28 elements, "
+                       "matrixgraph_b200/data/batch_seeds.json), count mode"}
+    for name, fn in (("per_query_reference", lambda: [dg.count(q) for q in qs]),
+                     ("batch_reference", lambda: dg.batch_count(qs).tolist()),
+                     ("batch_learned", lambda: dg.batch_count(qs, order="learned",
+                                                              model=model).tolist())):
+        fn()  # warm-up
+        t0 = time.perf_counter()
+        counts = fn()
+        wall = time.perf_counter() - t0
+        assert [int(c) for c in counts] == rec["counts"], name
+        out[name] = {"seconds": wall, "queries_per_s": len(qs) / wall}
+    base = out["per_query_reference"]["seconds"]
+    for name in ("batch_reference", "batch_learned"):
+        out[name]["speedup_vs_per_query_reference"] = base / out[name]["seconds"]
+    model.free()
+    return out
+
+
+def heldout_summary():
+    """Learned vs reference order on held-out 6-10-vertex queries, as recorded
+    by `python -m matrixgraph_b200.workloads eval-order` (not re-measured)."""
+    path = os.path.join(ROOT, "matrixgraph_b200", "data", "order_eval.json")
+    try:
+        with open(path) as f:
+            sm = json.load(f)["summary"]
+    except Exception:
+        return None
+    keep = ("n", "median_speedup_device", "geomean_speedup_device", "median_regret",
+            "total_ms_ref", "total_ms_learned")
+    return {"source": "matrixgraph_b200/data/order_eval.json", **{k: sm.get(k) for k in keep}}
+
+
 def run_mine(args):
     import torch
 
@@ -250,7 +280,7 @@ def run_mine(args):
     t0 = time.perf_counter()
     g, qs = workload(args.scale, args.queries)
     gen_s = time.perf_counter() - t0
-    buckets = first_bucket_sizes(g, qs)
+    buckets = mg.level0_sizes(g, qs)
     ranges = [mg.shard_roots(nb, rank, world) if world > 1 else None for nb in buckets]
     dg = mg.DeviceGraph(g, device)
     info = dg.info
@@ -332,6 +362,9 @@ def run_mine(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, _ = cpu_baseline(g, qs, args.cpu_seconds)
+    batch = None
+    if world == 1 and not args.no_batch and args.scale == 22:
+        batch = batched_workload(g, dg)
     if rank == 0:
         line = {"metric": "exact embeddings/s", "value": value, "unit": "embeddings/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -344,6 +377,7 @@ def run_mine(args):
                          "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                          "seconds_per_step": e2e_s} if e2e_times else None),
                 "clocks": clocks, "gpu_launches": launches * args.steps,
+                "batched": batch, "learned_order_heldout": heldout_summary(),
                 "graph": {"n": info["n"], "m_out": info["m_out"],
                           "device_bytes": info["device_bytes"], "max_degree": info["max_degree"],
                           "gen_seconds": gen_s}}

@@ -733,7 +733,10 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
     // Survivors that extend the prefix: append to the next level table.  One
     // reservation per tile keeps a tile's survivors (one row run, usually one
     // query) contiguous in the next table.
+    // Launches without an output table (last or closed-form positions) skip
+    // the reservation and its barriers.
     const bool wr = ok && !fin && !fused;
+    if (a.out_cap) {
     const uint32_t wm = __ballot_sync(FULL, wr);
     if (lane == 0) s_wcnt[threadIdx.x >> 5] = __popc(wm);
     __syncthreads();
@@ -759,6 +762,9 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
         }
       }
     }
+    } else if (wr) {
+      atomicOr(&a.ctr[C_ERR], (unsigned long long)ERR_OVERFLOW);  // no table to append to
+    }
     // Emit mode: complete matches as rows in query-vertex order.
     const bool em = ok && fin && !a.count_mode;
     const uint32_t emm = __ballot_sync(FULL, em);
@@ -779,7 +785,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
         }
       }
     }
-    __syncthreads();  // s_wcnt / s_wbase are reused by the next tile
+    if (a.out_cap) __syncthreads();  // s_wcnt / s_wbase are reused by the next tile
   }
   // Once per grab: fold the per-thread counts of a warp that holds one query.
   acc_flush_warp(a, cnt_q, i, cnt, s1, sk, false);

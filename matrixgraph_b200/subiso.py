@@ -157,6 +157,18 @@ class DeviceGraph:
             pass
 
 
+def level0_sizes(g: CSRGraph, qs: Sequence[CSRGraph], order="reference") -> list[int]:
+    """Level-0 candidates of each query: the label bucket of its first vertex."""
+    lab = g.array("labels")
+    vals, cnts = np.unique(lab, return_counts=True)
+    size = dict(zip(vals.tolist(), cnts.tolist()))
+    out = []
+    for q in qs:
+        first = plan_order(q, order=order)[0]
+        out.append(int(size.get(int(q.array("labels")[first]), 0)))
+    return out
+
+
 def shard_roots(n_roots: int, rank: int, world: int) -> tuple[int, int]:
     """Contiguous level-0 candidate range of one rank (independent shards)."""
     base, rem = divmod(n_roots, world)

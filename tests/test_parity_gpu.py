@@ -267,12 +267,13 @@ def test_batch_orders_level_rows_and_budget(c1):
     """Per-query orders and prefix counts in one batch equal the oracle's; a
     per-query budget marks only over-budget queries."""
     g, q, dg = c1
+    from matrixgraph_b200.order_model import random_connected_order
     rng = np.random.default_rng(11)
     qs, orders = [], []
     for i in range(24):
         x = mg.query_random(g, 3 + i % 5, 0.3, seed=3000 + i)
         qs.append(x)
-        orders.append(rng.permutation(x.n).tolist())
+        orders.append(random_connected_order(x, rng))
     counts, rows, _ = dg.batch_count_orders(qs, orders)
     for x, od, c, r in zip(qs, orders, counts, rows):
         want = oracle_count(g, x, order=od)
