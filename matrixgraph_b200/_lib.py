@@ -154,6 +154,21 @@ _SIGS = {
                                           C.POINTER(C.c_float), P32]),
 }
 
+# include/mg_gar_match.h
+_PI32 = C.POINTER(C.c_int32)
+_PI = C.POINTER(C.c_int)
+_GAR_ARGS = [P32, _PI32, C.c_int, P32, P32, P32, _PI32, C.c_int,        # data graph
+             _PI32, C.c_int, _PI32, _PI32, _PI32, C.c_int,              # pattern
+             _PI, P32, _PI32, _PI32, _PI32, _PI32, C.c_int, _PI,         # rows
+             P32, C.c_int, _PI]                                          # matched ids
+_SIGS["matrixgraph_gar_match"] = (C.c_int, list(_GAR_ARGS))
+_SIGS["mg_gar_match_ex"] = (C.c_int, list(_GAR_ARGS) + [C.POINTER(Opts), _PU64])
+_SIGS["mg_gar_instance"] = (C.c_int, [P32, _PI32, C.c_int, P32, P32, _PI32, C.c_int,
+                                      _PI32, C.c_int, _PI32, _PI32, _PI32, C.c_int,
+                                      _PV, _PVP, _PV, _PVP])
+_SIGS["mg_gar_flatten"] = (C.c_int, [P32, C.c_uint64, C.c_uint32, C.c_uint32, P32, C.c_int]
+                           + list(_GAR_ARGS[14:]))
+
 EXPORTED = tuple(_SIGS)
 
 for _name, (_res, _args) in _SIGS.items():

@@ -9,6 +9,7 @@
 // kernel_woj_subsio.cu:385-446) and label buckets (the level-0 candidate
 // ranges).
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 
@@ -484,6 +485,25 @@ int ensure_full_stats(DevGraph* dg) {
     S.label_nlb_density[l] = nl;
   }
   dg->stats_full = true;
+  return MG_OK;
+}
+
+// Device of an entry point that takes no device argument: the one named by
+// MATRIXGRAPH_CUDA_DEVICE when it is a valid index (the reference's
+// set_device_from_env, core/go_api/matrixgraph_go_api.cu:22-34), else the
+// calling thread's current device.  The current device is not changed.
+int env_or_current_device(int* dev) {
+  int count = 0;
+  MG_CK(cudaGetDeviceCount(&count));
+  const char* s = std::getenv("MATRIXGRAPH_CUDA_DEVICE");
+  if (s && s[0]) {
+    const int d = std::atoi(s);
+    if (d >= 0 && d < count) {
+      *dev = d;
+      return MG_OK;
+    }
+  }
+  MG_CK(cudaGetDevice(dev));
   return MG_OK;
 }
 

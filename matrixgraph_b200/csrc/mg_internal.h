@@ -104,6 +104,9 @@ bool order_is_permutation(const uint32_t* order, uint32_t k);
 // Learned order model (mg_order_model.cu).
 int order_learned(void* model, const QueryGraph& q, const GraphStats& gs,
                   uint32_t* order);
+// Device named by MATRIXGRAPH_CUDA_DEVICE, else the current one (mg_graph.cu).
+int env_or_current_device(int* dev);
+
 int order_learned_batch(void* model, const std::vector<const QueryGraph*>& qs,
                         const GraphStats& gs,
                         std::vector<std::array<uint32_t, MG_MAX_QUERY_VERTICES>>& orders);
