@@ -46,6 +46,7 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--queries", default="",
                    help="comma-separated subset of the query shapes (profiling runs)")
+    p.add_argument("--no-gar", action="store_true", help="skip the GAR match timing")
     p.add_argument("--no-batch", action="store_true",
                    help="skip the batched-workload measurement")
     return p.parse_args()
@@ -256,6 +257,44 @@ def batched_workload(g, dg):
     return out
 
 
+def gar_workload(reps=3):
+    """matrixgraph_gar_match end to end (host arrays in, grouped output back,
+    graph upload included) on an R-MAT scale-18 multigraph seen as directed
+    edges with 8 uniform vertex labels and 4 uniform edge labels: a tailed
+    triangle whose edges use three edge labels (subdivided instance) and the
+    same shape with one edge label."""
+    import numpy as np
+
+    import matrixgraph_b200 as mg
+    from matrixgraph_b200.gar import GARGraphArrays, GARPatternArrays, gar_match
+    g = mg.rmat(18, 16, 0.57, 0.19, 0.19, seed=0, n_labels=8, label_kind="uniform",
+                label_seed=1)
+    off = g.array("out_off").astype(np.int64)
+    src = np.repeat(np.arange(g.n, dtype=np.uint32), np.diff(off))
+    dst = g.array("out_edges").astype(np.uint32)
+    rng = np.random.default_rng(5)
+    ga = GARGraphArrays(v_id=(10 ** 6 + np.arange(g.n)).astype(np.uint32),
+                        v_label_idx=g.array("labels").astype(np.int32), e_src=src, e_dst=dst,
+                        e_label_idx=rng.integers(0, 4, len(src)).astype(np.int32))
+    out = {"workload": f"R-MAT scale 18 ({g.n} vertices, {len(src)} directed edges), 8 vertex "
+                       "labels, 4 edge labels; tailed triangle 0->1->2->0, 2->3; "
+                       "row capacity 2^20, id capacity 2^24; host arrays in and out"}
+    for name, elab in (("three_edge_labels", [0, 1, 0, 2]), ("one_edge_label", [0, 0, 0, 0])):
+        pa = GARPatternArrays(node_label_idx=np.array([0, 1, 2, 3], np.int32),
+                              edge_src=np.array([0, 1, 2, 2], np.int32),
+                              edge_dst=np.array([1, 2, 0, 3], np.int32),
+                              edge_label_idx=np.array(elab, np.int32))
+        gar_match(ga, pa, 1 << 20, 1 << 24)  # warm-up
+        times = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            r = gar_match(ga, pa, 1 << 20, 1 << 24)
+            times.append(time.perf_counter() - t0)
+        out[name] = {"seconds": statistics.median(times), "matches": r.n_matches,
+                     "rows": r.row_size, "ids": r.match_size}
+    return out
+
+
 def heldout_summary():
     """Learned vs reference order on held-out 6-10-vertex queries, as recorded
     by `python -m matrixgraph_b200.workloads eval-order` (not re-measured)."""
@@ -365,6 +404,12 @@ def run_mine(args):
     batch = None
     if world == 1 and not args.no_batch and args.scale == 22:
         batch = batched_workload(g, dg)
+    gar = None
+    if world == 1 and not args.no_gar:
+        try:
+            gar = gar_workload()
+        except Exception as e:  # reported in the line, the headline stands
+            gar = {"error": repr(e)}
     if rank == 0:
         line = {"metric": "exact embeddings/s", "value": value, "unit": "embeddings/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -377,7 +422,7 @@ def run_mine(args):
                          "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                          "seconds_per_step": e2e_s} if e2e_times else None),
                 "clocks": clocks, "gpu_launches": launches * args.steps,
-                "batched": batch, "learned_order_heldout": heldout_summary(),
+                "batched": batch, "learned_order_heldout": heldout_summary(), "gar_match": gar,
                 "graph": {"n": info["n"], "m_out": info["m_out"],
                           "device_bytes": info["device_bytes"], "max_degree": info["max_degree"],
                           "gen_seconds": gen_s}}
