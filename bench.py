@@ -28,6 +28,12 @@ import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+_T0 = time.perf_counter()
+
+
+def _log(stage: str) -> None:
+    """Stage timestamps on stderr (stdout carries only the JSON line)."""
+    print(f"[bench +{time.perf_counter() - _T0:7.1f}s] {stage}", file=sys.stderr, flush=True)
 sys.path.insert(0, ROOT)
 
 SHAPE_SEEDS = 2  # query i uses seed 2 + i
@@ -151,32 +157,101 @@ def dist_setup(args):
     return world, rank, local
 
 
+def _timed_count(og, oq, order, threads, root_range, limit_s):
+    """The oracle count of one root range in a forked child, killed (by its
+    pid) once ``limit_s`` has passed.  Returns (count, seconds measured in the
+    child) or None.  Only called before this process initialises CUDA."""
+    import select
+    import signal
+
+    import oracle as O
+    rfd, wfd = os.pipe()
+    pid = os.fork()
+    if pid == 0:
+        try:
+            os.close(rfd)
+            t0 = time.perf_counter()
+            res = O.count(og, oq, order=order, threads=threads, root_range=root_range)
+            dt = time.perf_counter() - t0
+            os.write(wfd, json.dumps([res["count"], dt]).encode())
+        finally:
+            os._exit(0)
+    os.close(wfd)
+    deadline = time.monotonic() + limit_s
+    data, eof = b"", False
+    while not eof:
+        left = deadline - time.monotonic()
+        if left <= 0:
+            break
+        ready, _, _ = select.select([rfd], [], [], left)
+        if ready:
+            chunk = os.read(rfd, 4096)
+            eof = not chunk
+            data += chunk
+    if not eof:
+        os.kill(pid, signal.SIGKILL)
+    os.waitpid(pid, 0)
+    os.close(rfd)
+    try:
+        count, dt = json.loads(data.decode())
+        return int(count), float(dt)
+    except ValueError:
+        return None
+
+
+def choose_sample(og, oq, order, nb, per_q, threads):
+    """A root range of one query whose oracle count takes about per_q / 4 to
+    per_q seconds: prefixes [0, r) with r = 1, 4, 16, ...; each attempt runs
+    under a hard limit, so a range that reaches a hub whose enumeration would
+    take minutes is abandoned and the previous range kept.  When even the
+    first root passes the limit, suffixes [nb - r, nb) (the low-degree end of
+    the bucket) are tried instead.  Returns (begin, end, count, seconds) or
+    None."""
+    limit = max(2.0, 2.0 * per_q)
+    for suffix in (False, True):
+        best, r = None, 1
+        while nb > 0:
+            rr = (nb - r, nb) if suffix else (0, r)
+            res = _timed_count(og, oq, order, threads, rr, limit)
+            if res is None:
+                break
+            best = (rr[0], rr[1], res[0], res[1])
+            if res[1] >= per_q / 4 or r >= nb:
+                break
+            r = min(nb, r * 4)
+        if best is not None:
+            return best
+    return None
+
+
+def _sample_text(samples):
+    return ", ".join("excluded (first and last root each over the limit)" if s is None else
+                     f"[{s[0]},{s[1]})/{s[4]}" for s in samples)
+
+
 def cpu_baseline(g, qs, target_s):
-    """The oracle (exact CPU port, all host threads) on a bounded sample of roots."""
+    """The oracle (exact CPU port, all host threads) on a bounded sample of
+    each query's level-0 candidates (see choose_sample).  Runs before this
+    process initialises CUDA."""
     import oracle as O
     threads = os.cpu_count() or 1
     og = O.Graph.from_csr(g)
-    total_c, total_t, parts = 0, 0.0, []
+    total_c, total_t, samples = 0, 0.0, []
     per_q = target_s / len(qs)
     for q in qs:
         oq = O.query_from_csr(q)
         order = O.reference_order(oq)
         nb = O.bucket_size(og, oq, order)
-        r = max(1, nb // 4096)
-        while True:
-            t0 = time.perf_counter()
-            res = O.count(og, oq, order=order, threads=threads, root_range=(0, r))
-            dt = time.perf_counter() - t0
-            if dt >= per_q / 4 or r >= nb:
-                break
-            r = min(nb, r * 4)
-        total_c += res["count"]
-        total_t += dt
-        parts.append(f"{r}/{nb}")
+        s = choose_sample(og, oq, order, nb, per_q, threads)
+        samples.append(None if s is None else s + (nb,))
+        if s is not None:
+            total_c += s[2]
+            total_t += s[3]
     return {"value": total_c / total_t if total_t > 0 else 0.0, "unit": "embeddings/s",
             "cores": threads, "kind": "port",
-            "sample": "oracle over the first r of each query's level-0 candidates (r/total: "
-                      + ", ".join(parts) + "), embeddings counted / wall seconds"}, og
+            "sample": "oracle over a root range [begin, end) of each query's level-0 "
+                      "candidates out of the bucket size (" + _sample_text(samples) +
+                      "), embeddings counted / wall seconds"}, og
 
 
 def run_reference(args):
@@ -194,28 +269,27 @@ def run_reference(args):
     for oq in oqs:
         order = O.reference_order(oq)
         nb = O.bucket_size(og, oq, order)
-        r = max(1, nb // 4096)
-        while True:
-            t0 = time.perf_counter()
-            O.count(og, oq, order=order, threads=threads, root_range=(0, r))
-            if time.perf_counter() - t0 >= per_q / 4 or r >= nb:
-                break
-            r = min(nb, r * 4)
-        samples.append((order, r, nb))
+        s = choose_sample(og, oq, order, nb, per_q, threads)
+        samples.append(None if s is None else s + (nb, order))
     for _ in range(max(0, args.warmup - 1)):
-        pass
+        for oq, smp in zip(oqs, samples):
+            if smp is not None:
+                O.count(og, oq, order=smp[5], threads=threads, root_range=(smp[0], smp[1]))
     times, counts = [], 0
     for _ in range(args.steps):
         t0 = time.perf_counter()
         c = 0
-        for oq, (order, r, nb) in zip(oqs, samples):
-            c += O.count(og, oq, order=order, threads=threads, root_range=(0, r))["count"]
+        for oq, smp in zip(oqs, samples):
+            if smp is not None:
+                c += O.count(og, oq, order=smp[5], threads=threads,
+                             root_range=(smp[0], smp[1]))["count"]
         times.append(time.perf_counter() - t0)
         counts = c
     ms = 1e3 * statistics.mean(times)
-    value = counts / (ms / 1e3)
-    sample = ("oracle (exact CPU port of the reference algorithm) over the first r of each "
-              "query's level-0 candidates: " + ", ".join(f"{r}/{nb}" for _, r, nb in samples))
+    value = counts / (ms / 1e3) if ms > 0 else 0.0
+    sample = ("oracle (exact CPU port of the reference algorithm) over a root range "
+              "[begin, end) of each query's level-0 candidates out of the bucket size: "
+              + _sample_text(samples))
     line = {"impl": "reference", "metric": "exact embeddings/s", "value": value,
             "unit": "embeddings/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -250,6 +324,7 @@ def batched_workload(g, dg):
         wall = time.perf_counter() - t0
         assert [int(c) for c in counts] == rec["counts"], name
         out[name] = {"seconds": wall, "queries_per_s": len(qs) / wall}
+        _log(f"batched {name}: {wall:.2f} s")
     base = out["per_query_reference"]["seconds"]
     for name in ("batch_reference", "batch_learned"):
         out[name]["speedup_vs_per_query_reference"] = base / out[name]["seconds"]
@@ -292,6 +367,7 @@ def gar_workload(reps=3):
             times.append(time.perf_counter() - t0)
         out[name] = {"seconds": statistics.median(times), "matches": r.n_matches,
                      "rows": r.row_size, "ids": r.match_size}
+        _log(f"gar {name}: {out[name]['seconds']:.2f} s")
     return out
 
 
@@ -315,14 +391,21 @@ def run_mine(args):
     import matrixgraph_b200 as mg
     world, rank, local = dist_setup(args)
     device = local
-    torch.cuda.set_device(device)
     t0 = time.perf_counter()
     g, qs = workload(args.scale, args.queries)
     gen_s = time.perf_counter() - t0
+    _log("workload generated")
+    # The CPU baseline forks its oracle runs, so it goes before CUDA starts.
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu, _ = cpu_baseline(g, qs, args.cpu_seconds)
+        _log("cpu baseline done")
+    torch.cuda.set_device(device)
     buckets = mg.level0_sizes(g, qs)
     ranges = [mg.shard_roots(nb, rank, world) if world > 1 else None for nb in buckets]
     dg = mg.DeviceGraph(g, device)
     info = dg.info
+    _log("graph uploaded")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device=f"cuda:{device}")
 
     def step(collect):
@@ -355,6 +438,7 @@ def run_mine(args):
     if world > 1:
         torch.distributed.barrier()
     clocks = clk.stop()
+    _log("timed steps done")
     ms_step = statistics.mean(r[0] for r in recs)
     counts = recs[-1][4]
     launches = recs[-1][1]
@@ -386,6 +470,7 @@ def run_mine(args):
         dg2.free()
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = statistics.median(e2e_times) if e2e_times else float("nan")
+    _log("end-to-end runs done")
     if world > 1:
         t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{device}")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -398,16 +483,15 @@ def run_mine(args):
                 "basis": f"B_alg (count-mode definition) per step / device time per step; "
                          f"peak {peak_kind} copy bandwidth",
                 "balg_count_bytes_per_step": balgc, "balg_bytes_per_step": balg}
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu, _ = cpu_baseline(g, qs, args.cpu_seconds)
     batch = None
     if world == 1 and not args.no_batch and args.scale == 22:
         batch = batched_workload(g, dg)
+        _log("batched workload done")
     gar = None
     if world == 1 and not args.no_gar:
         try:
             gar = gar_workload()
+            _log("gar workload done")
         except Exception as e:  # reported in the line, the headline stands
             gar = {"error": repr(e)}
     if rank == 0:

@@ -103,7 +103,7 @@ class Graph:
         return {"n": n.value, "L": L.value, "symmetric": bool(s.value), "m_out": m.value}
 
     def __del__(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and _lib is not None:  # _lib is None at interpreter exit
             _lib.orc_graph_free(self.h)
             self.h = None
 
