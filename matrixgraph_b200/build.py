@@ -103,7 +103,8 @@ def _build_host(nvcc: str) -> None:
     hdrs = [os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith(".h")]
     if not srcs:
         return
-    if not _stale(EXE, srcs + hdrs + [os.path.join(INCLUDE, "mg_subiso.h"), LIB]):
+    incs = [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
+    if not _stale(EXE, srcs + hdrs + incs + [LIB]):
         return
     _run(["g++"] + CXX_FLAGS + ["-I", HOST] + srcs + ["-o", EXE, "-L", PKG, "-lmg_subiso",
                                                        "-Wl,-rpath,$ORIGIN"])

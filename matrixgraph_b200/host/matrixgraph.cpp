@@ -72,9 +72,47 @@ void SubIso::Write() const {
   }
 }
 
+int GARMatch::Run(const uint32_t* g_v_id, const int32_t* g_v_label_idx, int g_n_vertices,
+                  const uint32_t* g_e_src, const uint32_t* g_e_dst, const uint32_t* g_e_id,
+                  const int32_t* g_e_label_idx, int g_n_edges, const int32_t* p_node_label_idx,
+                  int p_n_nodes, const int32_t* p_edge_src, const int32_t* p_edge_dst,
+                  const int32_t* p_edge_label_idx, int p_n_edges, int* out_num_conditions,
+                  uint32_t* out_row_pivot_id, int32_t* out_row_cond_j, int32_t* out_row_pos,
+                  int32_t* out_row_offset, int32_t* out_row_count, int out_row_capacity,
+                  int* out_row_size, uint32_t* out_matched_v_ids, int out_match_capacity,
+                  int* out_match_size) {
+  return matrixgraph_gar_match(g_v_id, g_v_label_idx, g_n_vertices, g_e_src, g_e_dst, g_e_id,
+                               g_e_label_idx, g_n_edges, p_node_label_idx, p_n_nodes,
+                               p_edge_src, p_edge_dst, p_edge_label_idx, p_n_edges,
+                               out_num_conditions, out_row_pivot_id, out_row_cond_j,
+                               out_row_pos, out_row_offset, out_row_count, out_row_capacity,
+                               out_row_size, out_matched_v_ids, out_match_capacity,
+                               out_match_size);
+}
+
+void GARMatch::Run() {
+  if (!out_) {  // the reference's wrapper returns 1 without an output object
+    status_ = 1;
+    return;
+  }
+  status_ = Run(g_.v_id, g_.v_label_idx, g_.n_vertices, g_.e_src, g_.e_dst, g_.e_id,
+                g_.e_label_idx, g_.n_edges, p_.node_label_idx, p_.n_nodes, p_.edge_src,
+                p_.edge_dst, p_.edge_label_idx, p_.n_edges, out_->num_conditions,
+                out_->row_pivot_id, out_->row_cond_j, out_->row_pos, out_->row_offset,
+                out_->row_count, out_->row_capacity, out_->row_size, out_->matched_v_ids,
+                out_->match_capacity, out_->match_size);
+  if (status_ != MG_OK) std::cerr << "[GARMatch] " << mg_last_error() << std::endl;
+}
+
 void MatrixGraph::Run(TaskType type, SubIso* task) {
   (void)scheduler_;
-  if (type != kSubIso) throw Error(MG_E_ARG, "only kSubIso is served");
+  if (type != kSubIso) throw Error(MG_E_ARG, "a SubIso task needs kSubIso");
+  task->Run();
+}
+
+void MatrixGraph::Run(TaskType type, GARMatch* task) {
+  (void)scheduler_;
+  if (type != kGARMatch) throw Error(MG_E_ARG, "a GARMatch task needs kGARMatch");
   task->Run();
 }
 

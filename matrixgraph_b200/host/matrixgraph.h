@@ -5,6 +5,8 @@
 //          output_path).Run()         core/task/gpu_task/subiso.cuh:43-51
 //   MatrixGraph(scheduler).Run(kSubIso, task)
 //                                     core/matrixgraph.cuh:36-42, matrixgraph.cu:30-46
+//   GARMatch(g, p, out).Run(), GARMatch::Run(arrays...)
+//                                     core/task/gpu_task/gar_match.cuh:33-70
 //
 // Differences from the reference: the count is exact; errors raise
 // std::runtime_error with the library's message instead of exiting.
@@ -15,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "mg_gar_match.h"
 #include "mg_subiso.h"
 
 namespace matrixgraph {
@@ -62,10 +65,80 @@ class SubIso {
   double match_ms_ = 0;
 };
 
+// GAR match over serialized arrays: the reference's GARGraphArrays,
+// GARPatternArrays and GARMatchArrays (core/data_structures/
+// gar_graph_arrays.h, gar_pattern_arrays.h, gar_match_arrays.h:56-70) and
+// the array-based GARMatch task (core/task/gpu_task/gar_match.cuh:33-70).
+// The config-file constructor of the reference (an ArangoDB loader) has no
+// counterpart here.
+struct GARGraphArrays {
+  const uint32_t* v_id = nullptr;
+  const int32_t* v_label_idx = nullptr;
+  int n_vertices = 0;
+  const uint32_t* e_src = nullptr;
+  const uint32_t* e_dst = nullptr;
+  const uint32_t* e_id = nullptr;
+  const int32_t* e_label_idx = nullptr;
+  int n_edges = 0;
+};
+
+struct GARPatternArrays {
+  const int32_t* node_label_idx = nullptr;
+  int n_nodes = 0;
+  const int32_t* edge_src = nullptr;
+  const int32_t* edge_dst = nullptr;
+  const int32_t* edge_label_idx = nullptr;
+  int n_edges = 0;
+};
+
+struct GARMatchArrays {
+  int* num_conditions = nullptr;
+  uint32_t* row_pivot_id = nullptr;
+  int32_t* row_cond_j = nullptr;
+  int32_t* row_pos = nullptr;
+  int32_t* row_offset = nullptr;
+  int32_t* row_count = nullptr;
+  int row_capacity = 0;
+  int* row_size = nullptr;
+  uint32_t* matched_v_ids = nullptr;
+  int match_capacity = 0;
+  int* match_size = nullptr;
+};
+
+class GARMatch {
+ public:
+  GARMatch(const GARGraphArrays& g, const GARPatternArrays& p, GARMatchArrays* out)
+      : g_(g), p_(p), out_(out) {}
+
+  // C-style entry (the reference's static GARMatch::Run): 0 on success.
+  static int Run(const uint32_t* g_v_id, const int32_t* g_v_label_idx, int g_n_vertices,
+                 const uint32_t* g_e_src, const uint32_t* g_e_dst, const uint32_t* g_e_id,
+                 const int32_t* g_e_label_idx, int g_n_edges, const int32_t* p_node_label_idx,
+                 int p_n_nodes, const int32_t* p_edge_src, const int32_t* p_edge_dst,
+                 const int32_t* p_edge_label_idx, int p_n_edges, int* out_num_conditions,
+                 uint32_t* out_row_pivot_id, int32_t* out_row_cond_j, int32_t* out_row_pos,
+                 int32_t* out_row_offset, int32_t* out_row_count, int out_row_capacity,
+                 int* out_row_size, uint32_t* out_matched_v_ids, int out_match_capacity,
+                 int* out_match_size);
+
+  // Matches the arrays given at construction; the status is kept in
+  // Status() (0 on success, an MG_E_* code otherwise) instead of ending the
+  // process on a CUDA error.
+  void Run();
+  int Status() const { return status_; }
+
+ private:
+  GARGraphArrays g_;
+  GARPatternArrays p_;
+  GARMatchArrays* out_;
+  int status_ = 1;
+};
+
 class MatrixGraph {
  public:
   explicit MatrixGraph(SchedulerType scheduler = kCHBL) : scheduler_(scheduler) {}
   void Run(TaskType type, SubIso* task);
+  void Run(TaskType type, GARMatch* task);
 
  private:
   SchedulerType scheduler_;  // accepted and ignored by subiso, as in the reference
