@@ -118,3 +118,24 @@ def test_empty_results():
     # data edge labels absent: pattern edge labels are not compared
     g2 = GarGraph(g.v_id, g.v_label, g.e_src, g.e_dst, None, g.n_vertices)
     assert gar_match(g2, GarPattern([0, 1], [0], [1], [6], 2), 10, 10).n_embeddings == 3
+
+
+def test_restated_helpers_match_the_reference_build():
+    """The heap, popcount and label hash of oracle/gar.py against outputs of
+    the reference's own headers (tests/golden/make_gar_golden.py)."""
+    import json
+    import os
+
+    from oracle.gar import _hash_table
+    path = os.path.join(os.path.dirname(__file__), "golden", "gar_helpers.json")
+    ref = json.load(open(path))
+    assert [_hash_table(k) for k in range(len(ref["hash"]))] == ref["hash"]
+    for x, c in ref["count"]:
+        assert _bitmap_count(x) == c, x
+    assert len(ref["heap"]) == 300
+    for case in ref["heap"]:
+        h = _Heap()
+        for v in case["in"]:
+            h.insert(v)
+        assert h.offset == case["offset"]
+        assert h.data[:h.offset] == case["data"], case["in"]
