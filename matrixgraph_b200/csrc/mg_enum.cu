@@ -644,151 +644,151 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
   __shared__ uint32_t s_wcnt[EXPAND_BLOCK / 32];
   const uint64_t grab = a.grab ? a.grab : 4;
   for (;;) {
-  if (threadIdx.x == 0) s_base = atomicAdd(&a.ctr[C_TILE], (unsigned long long)grab);
-  __syncthreads();
-  const uint64_t gbase = s_base;
-  __syncthreads();
-  if (gbase >= ntiles) break;
-  const uint64_t gend = min(gbase + grab, ntiles);
-  for (uint64_t tile = gbase; tile < gend; ++tile) {
-    const uint64_t tb = a.t0 + tile * EXPAND_BLOCK;
-    const uint64_t te = min(tb + EXPAND_BLOCK, a.t1);
-    const uint32_t rlo = __ldg(a.tile_row + tile), rhi = __ldg(a.tile_row + tile + 1);
-    const uint64_t t = tb + threadIdx.x;
-    const bool valid = t < te;
-    bool ok = false, fin = false, fused = false;
-    uint32_t r = 0, x = 0, q = 0;
-    if (valid) {
-      r = find_row(a.woff, rlo, rhi, t);
-      const uint32_t e = uint32_t(t - a.woff[r]);
-      const uint8_t ci = a.dci[r];
-      const uint32_t ds = a.dstart[r];
-      q = a.in.qid ? a.in.qid[r] : 0u;
-      const PlanDev& P = a.plans[q];
-      const uint32_t lab = P.label[i];
-      uint32_t ddir = 0;
-      if (ci == DCI_BUCKET) {
-        x = __ldg(g.bucket_vid + ds + e);
-      } else {
-        ddir = P.cons[i][ci] >> 8;
-        x = __ldg(g.adj[ddir] + ds + e);
-      }
-      ok = true;
-      // injectivity: only earlier positions with the same label can collide
-      for (uint32_t m = P.samelab[i]; m && ok; m &= m - 1) {
-        const uint32_t j = __ffs(m) - 1;
-        if (a.in.col[j][r] == x) ok = false;
-      }
-      // remaining backward neighbours: binary search in their label slices
-      const uint32_t nc = P.ncons[i];
-      for (uint32_t c = 0; c < nc && ok; ++c) {
-        if (c == ci) continue;
-        const uint32_t cs = P.cons[i][c];
-        const uint32_t y = a.in.col[cs & 0xFF][r];
-        uint32_t s, en;
-        slice_of(g, cs >> 8, y, lab, s, en);
-        ok = contains(g.adj[cs >> 8], s, en, x);
-      }
-      if (ok && ((P.selfloop_mask >> i) & 1u)) ok = has_self(g, x);
-      fin = (i + 1 == P.k);
-      fused = !fin && a.count_mode && (i + 2 == P.k) && P.last_o1;
-      // Filters prune positions whose survivors are extended further; the
-      // position before a last position counted in closed form is not
-      // filtered (the closed form already yields 0 for hopeless candidates).
-      if (ok && !fin && a.filters && !(i + 2 == P.k && P.last_o1))
-        ok = pass_filters(g, P, i, x, a.filters);
-      if (ok) {
-        if (q != cnt_q) {
-          acc_flush(a, cnt_q, i, cnt, s1, sk);
-          cnt = s1 = sk = 0;
-          cnt_q = q;
+    if (threadIdx.x == 0) s_base = atomicAdd(&a.ctr[C_TILE], (unsigned long long)grab);
+    __syncthreads();
+    const uint64_t gbase = s_base;
+    __syncthreads();
+    if (gbase >= ntiles) break;
+    const uint64_t gend = min(gbase + grab, ntiles);
+    for (uint64_t tile = gbase; tile < gend; ++tile) {
+      const uint64_t tb = a.t0 + tile * EXPAND_BLOCK;
+      const uint64_t te = min(tb + EXPAND_BLOCK, a.t1);
+      const uint32_t rlo = __ldg(a.tile_row + tile), rhi = __ldg(a.tile_row + tile + 1);
+      const uint64_t t = tb + threadIdx.x;
+      const bool valid = t < te;
+      bool ok = false, fin = false, fused = false;
+      uint32_t r = 0, x = 0, q = 0;
+      if (valid) {
+        r = find_row(a.woff, rlo, rhi, t);
+        const uint32_t e = uint32_t(t - a.woff[r]);
+        const uint8_t ci = a.dci[r];
+        const uint32_t ds = a.dstart[r];
+        q = a.in.qid ? a.in.qid[r] : 0u;
+        const PlanDev& P = a.plans[q];
+        const uint32_t lab = P.label[i];
+        uint32_t ddir = 0;
+        if (ci == DCI_BUCKET) {
+          x = __ldg(g.bucket_vid + ds + e);
+        } else {
+          ddir = P.cons[i][ci] >> 8;
+          x = __ldg(g.adj[ddir] + ds + e);
         }
-        s1 += 1;
-        if (fin) {
-          if (a.count_mode) cnt += 1;
-        } else if (fused) {
-          const uint32_t kl = P.k - 1;
-          const uint32_t cs = P.cons[kl][0];
-          const uint32_t pos = cs & 0xFF, dir = cs >> 8;
-          const uint32_t y = pos == i ? x : a.in.col[pos][r];
+        ok = true;
+        // injectivity: only earlier positions with the same label can collide
+        for (uint32_t m = P.samelab[i]; m && ok; m &= m - 1) {
+          const uint32_t j = __ffs(m) - 1;
+          if (a.in.col[j][r] == x) ok = false;
+        }
+        // remaining backward neighbours: binary search in their label slices
+        const uint32_t nc = P.ncons[i];
+        for (uint32_t c = 0; c < nc && ok; ++c) {
+          if (c == ci) continue;
+          const uint32_t cs = P.cons[i][c];
+          const uint32_t y = a.in.col[cs & 0xFF][r];
           uint32_t s, en;
-          slice_of(g, dir, y, P.label[kl], s, en);
-          unsigned long long c1 = en - s;
-          bal += 8ull + 4ull * c1;
-          balc += 8ull;
-          for (uint32_t m = P.samelab[kl]; m; m &= m - 1) {
-            const uint32_t j = __ffs(m) - 1;
-            if ((P.guar[kl] >> j) & 1u) {
-              c1 -= 1;
+          slice_of(g, cs >> 8, y, lab, s, en);
+          ok = contains(g.adj[cs >> 8], s, en, x);
+        }
+        if (ok && ((P.selfloop_mask >> i) & 1u)) ok = has_self(g, x);
+        fin = (i + 1 == P.k);
+        fused = !fin && a.count_mode && (i + 2 == P.k) && P.last_o1;
+        // Filters prune positions whose survivors are extended further; the
+        // position before a last position counted in closed form is not
+        // filtered (the closed form already yields 0 for hopeless candidates).
+        if (ok && !fin && a.filters && !(i + 2 == P.k && P.last_o1))
+          ok = pass_filters(g, P, i, x, a.filters);
+        if (ok) {
+          if (q != cnt_q) {
+            acc_flush(a, cnt_q, i, cnt, s1, sk);
+            cnt = s1 = sk = 0;
+            cnt_q = q;
+          }
+          s1 += 1;
+          if (fin) {
+            if (a.count_mode) cnt += 1;
+          } else if (fused) {
+            const uint32_t kl = P.k - 1;
+            const uint32_t cs = P.cons[kl][0];
+            const uint32_t pos = cs & 0xFF, dir = cs >> 8;
+            const uint32_t y = pos == i ? x : a.in.col[pos][r];
+            uint32_t s, en;
+            slice_of(g, dir, y, P.label[kl], s, en);
+            unsigned long long c1 = en - s;
+            bal += 8ull + 4ull * c1;
+            balc += 8ull;
+            for (uint32_t m = P.samelab[kl]; m; m &= m - 1) {
+              const uint32_t j = __ffs(m) - 1;
+              if ((P.guar[kl] >> j) & 1u) {
+                c1 -= 1;
+              } else {
+                const uint32_t mj = j == i ? x : a.in.col[j][r];
+                c1 -= contains(g.adj[dir], s, en, mj) ? 1ull : 0ull;
+              }
+            }
+            sk += c1;
+            cnt += c1;
+          }
+        }
+      }
+      // Survivors that extend the prefix: append to the next level table.  One
+      // reservation per tile keeps a tile's survivors (one row run, usually one
+      // query) contiguous in the next table.
+      // Launches without an output table (last or closed-form positions) skip
+      // the reservation and its barriers.
+      const bool wr = ok && !fin && !fused;
+      if (a.out_cap) {
+        const uint32_t wm = __ballot_sync(FULL, wr);
+        if (lane == 0) s_wcnt[threadIdx.x >> 5] = __popc(wm);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          uint32_t tot = 0;
+          for (uint32_t w = 0; w < EXPAND_BLOCK / 32; ++w) {
+            const uint32_t c = s_wcnt[w];
+            s_wcnt[w] = tot;
+            tot += c;
+          }
+          s_wbase = tot ? atomicAdd(&a.ctr[C_OUT], (unsigned long long)tot) : 0ull;
+        }
+        __syncthreads();
+        if (wm) {
+          if (wr) {
+            const unsigned long long idx = s_wbase + s_wcnt[threadIdx.x >> 5] + __popc(wm & lanemask_lt());
+            if (idx < a.out_cap) {
+              for (uint32_t j = 0; j < i; ++j) a.out.col[j][idx] = a.in.col[j][r];
+              a.out.col[i][idx] = x;
+              if (a.out.qid) a.out.qid[idx] = q;
             } else {
-              const uint32_t mj = j == i ? x : a.in.col[j][r];
-              c1 -= contains(g.adj[dir], s, en, mj) ? 1ull : 0ull;
+              atomicOr(&a.ctr[C_ERR], (unsigned long long)ERR_OVERFLOW);
             }
           }
-          sk += c1;
-          cnt += c1;
+        }
+      } else if (wr) {
+        atomicOr(&a.ctr[C_ERR], (unsigned long long)ERR_OVERFLOW);  // no table to append to
+      }
+      // Emit mode: complete matches as rows in query-vertex order.
+      const bool em = ok && fin && !a.count_mode;
+      const uint32_t emm = __ballot_sync(FULL, em);
+      if (emm) {
+        const uint32_t leader = __ffs(emm) - 1;
+        unsigned long long base = 0;
+        if (lane == leader) base = atomicAdd(&a.ctr[C_EMIT], (unsigned long long)__popc(emm));
+        base = __shfl_sync(FULL, base, leader);
+        if (em) {
+          const unsigned long long idx = base + __popc(emm & lanemask_lt());
+          if (idx < a.emit_cap) {
+            const PlanDev& P = a.plans[q];
+            for (uint32_t j = 0; j < i; ++j)
+              a.emit_col[P.perm[j]][idx] = __ldg(g.globalid + a.in.col[j][r]);
+            a.emit_col[P.perm[i]][idx] = __ldg(g.globalid + x);
+          } else {
+            atomicOr(&a.ctr[C_ERR], (unsigned long long)ERR_OVERFLOW);
+          }
         }
       }
+      if (a.out_cap) __syncthreads();  // s_wcnt / s_wbase are reused by the next tile
     }
-    // Survivors that extend the prefix: append to the next level table.  One
-    // reservation per tile keeps a tile's survivors (one row run, usually one
-    // query) contiguous in the next table.
-    // Launches without an output table (last or closed-form positions) skip
-    // the reservation and its barriers.
-    const bool wr = ok && !fin && !fused;
-    if (a.out_cap) {
-    const uint32_t wm = __ballot_sync(FULL, wr);
-    if (lane == 0) s_wcnt[threadIdx.x >> 5] = __popc(wm);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      uint32_t tot = 0;
-      for (uint32_t w = 0; w < EXPAND_BLOCK / 32; ++w) {
-        const uint32_t c = s_wcnt[w];
-        s_wcnt[w] = tot;
-        tot += c;
-      }
-      s_wbase = tot ? atomicAdd(&a.ctr[C_OUT], (unsigned long long)tot) : 0ull;
-    }
-    __syncthreads();
-    if (wm) {
-      if (wr) {
-        const unsigned long long idx = s_wbase + s_wcnt[threadIdx.x >> 5] + __popc(wm & lanemask_lt());
-        if (idx < a.out_cap) {
-          for (uint32_t j = 0; j < i; ++j) a.out.col[j][idx] = a.in.col[j][r];
-          a.out.col[i][idx] = x;
-          if (a.out.qid) a.out.qid[idx] = q;
-        } else {
-          atomicOr(&a.ctr[C_ERR], (unsigned long long)ERR_OVERFLOW);
-        }
-      }
-    }
-    } else if (wr) {
-      atomicOr(&a.ctr[C_ERR], (unsigned long long)ERR_OVERFLOW);  // no table to append to
-    }
-    // Emit mode: complete matches as rows in query-vertex order.
-    const bool em = ok && fin && !a.count_mode;
-    const uint32_t emm = __ballot_sync(FULL, em);
-    if (emm) {
-      const uint32_t leader = __ffs(emm) - 1;
-      unsigned long long base = 0;
-      if (lane == leader) base = atomicAdd(&a.ctr[C_EMIT], (unsigned long long)__popc(emm));
-      base = __shfl_sync(FULL, base, leader);
-      if (em) {
-        const unsigned long long idx = base + __popc(emm & lanemask_lt());
-        if (idx < a.emit_cap) {
-          const PlanDev& P = a.plans[q];
-          for (uint32_t j = 0; j < i; ++j)
-            a.emit_col[P.perm[j]][idx] = __ldg(g.globalid + a.in.col[j][r]);
-          a.emit_col[P.perm[i]][idx] = __ldg(g.globalid + x);
-        } else {
-          atomicOr(&a.ctr[C_ERR], (unsigned long long)ERR_OVERFLOW);
-        }
-      }
-    }
-    if (a.out_cap) __syncthreads();  // s_wcnt / s_wbase are reused by the next tile
-  }
-  // Once per grab: fold the per-thread counts of a warp that holds one query.
-  acc_flush_warp(a, cnt_q, i, cnt, s1, sk, false);
+    // Once per grab: fold the per-thread counts of a warp that holds one query.
+    acc_flush_warp(a, cnt_q, i, cnt, s1, sk, false);
   }  // grab loop
   acc_flush_warp(a, cnt_q, i, cnt, s1, sk, true);
   bal = warp_sum(bal);
