@@ -200,7 +200,7 @@ def _timed_count(og, oq, order, threads, root_range, limit_s):
 
 
 def choose_sample(og, oq, order, nb, per_q, threads):
-    """A root range of one query whose oracle count takes about per_q / 4 to
+    """A root range of one query whose oracle count takes about per_q / 2 to
     per_q seconds: prefixes [0, r) with r = 1, 4, 16, ...; each attempt runs
     under a hard limit, so a range that reaches a hub whose enumeration would
     take minutes is abandoned and the previous range kept.  When even the
@@ -216,7 +216,7 @@ def choose_sample(og, oq, order, nb, per_q, threads):
             if res is None:
                 break
             best = (rr[0], rr[1], res[0], res[1])
-            if res[1] >= per_q / 4 or r >= nb:
+            if res[1] >= per_q / 2 or r >= nb:
                 break
             r = min(nb, r * 4)
         if best is not None:
