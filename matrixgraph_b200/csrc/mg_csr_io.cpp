@@ -391,6 +391,42 @@ static void parallel_for(uint64_t n, F f, unsigned threads = 0) {
   for (auto& t : ts) t.join();
 }
 
+// Vertex ranges of about equal weight (list entries plus one per vertex,
+// from the prefix offsets off64), handed out dynamically: hub-heavy id
+// ranges (R-MAT ids are not permuted) no longer land on one thread.
+template <class F>
+static void parallel_for_volume(const std::vector<uint64_t>& off64, uint32_t n, F f) {
+  const unsigned threads = hw_threads();
+  const uint64_t total = off64[n] + n;
+  if (total < 65536 || threads == 1) {
+    f(0, n);
+    return;
+  }
+  const uint32_t chunks = threads * 16;
+  std::vector<uint32_t> bound(chunks + 1, n);
+  bound[0] = 0;
+  for (uint32_t c = 1; c < chunks; ++c) {
+    const uint64_t target = total * c / chunks;
+    uint32_t lo = bound[c - 1], hi = n;  // first v with off64[v] + v >= target
+    while (lo < hi) {
+      const uint32_t mid = lo + (hi - lo) / 2;
+      if (off64[mid] + mid < target)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    bound[c] = lo;
+  }
+  std::atomic<uint32_t> next{0};
+  std::vector<std::thread> ts;
+  for (unsigned t = 0; t < threads; ++t)
+    ts.emplace_back([&]() {
+      for (uint32_t c; (c = next.fetch_add(1)) < chunks;)
+        if (bound[c] < bound[c + 1]) f(bound[c], bound[c + 1]);
+    });
+  for (auto& t : ts) t.join();
+}
+
 // One direction: CSR of (key -> val) pairs, sorted lists, optional dedup.
 static int build_dir(uint32_t n, const uint32_t* key, const uint32_t* val,
                      uint64_t m, bool sym, uint32_t flags,
@@ -425,7 +461,7 @@ static int build_dir(uint32_t n, const uint32_t* key, const uint32_t* val,
   });
   // Sort (and optionally dedupe) each list; vertices split by edge volume.
   std::vector<uint32_t> newdeg(n);
-  parallel_for(n, [&](uint64_t a, uint64_t b, unsigned) {
+  parallel_for_volume(off64, n, [&](uint64_t a, uint64_t b) {
     for (uint64_t v = a; v < b; ++v) {
       uint32_t* p = tmp.data() + off64[v];
       uint32_t* q = tmp.data() + off64[v + 1];
@@ -445,7 +481,7 @@ static int build_dir(uint32_t n, const uint32_t* key, const uint32_t* val,
     return MG_OK;
   }
   adj.resize(acc);
-  parallel_for(n, [&](uint64_t a, uint64_t b, unsigned) {
+  parallel_for_volume(off64, n, [&](uint64_t a, uint64_t b) {
     for (uint64_t v = a; v < b; ++v)
       std::memcpy(adj.data() + off[v], tmp.data() + off64[v], uint64_t(newdeg[v]) * 4);
   });
@@ -455,10 +491,21 @@ static int build_dir(uint32_t n, const uint32_t* key, const uint32_t* val,
 int build_csr_from_pairs(uint32_t n, const uint32_t* src, const uint32_t* dst,
                          uint64_t m, const uint32_t* labels, uint32_t flags,
                          HostCSR* g) {
-  for (uint64_t e = 0; e < m; ++e)
-    if (src[e] >= n || dst[e] >= n)
-      return set_error(MG_E_ARG, "edge %llu (%u,%u) out of range n=%u",
-                       (unsigned long long)e, src[e], dst[e], n);
+  std::atomic<uint64_t> bad{m};  // first edge with an endpoint out of range
+  parallel_for(m, [&](uint64_t a, uint64_t b, unsigned) {
+    for (uint64_t e = a; e < b; ++e)
+      if (src[e] >= n || dst[e] >= n) {
+        uint64_t cur = bad.load();
+        while (e < cur && !bad.compare_exchange_weak(cur, e)) {
+        }
+        return;
+      }
+  });
+  if (bad.load() < m) {
+    const uint64_t e = bad.load();
+    return set_error(MG_E_ARG, "edge %llu (%u,%u) out of range n=%u", (unsigned long long)e,
+                     src[e], dst[e], n);
+  }
   const bool sym = flags & MG_BUILD_SYMMETRIZE;
   int rc = build_dir(n, src, dst, m, sym, flags, g->out_off, g->out_edges);
   if (rc) return rc;
