@@ -12,12 +12,13 @@ void Check(int rc) {
 
 SubIso::SubIso(const std::string& pattern_path, const std::string& data_graph_path,
                const std::string& data_graph_edgelist_path, const std::string& output_path,
-               const std::string& mode, int order, int device)
+               const std::string& mode, int order, int device, const std::string& model_path)
     : pattern_path_(pattern_path),
       data_graph_path_(data_graph_path),
       data_graph_edgelist_path_(data_graph_edgelist_path),
       output_path_(output_path),
       mode_(mode),
+      model_path_(model_path),
       order_(order),
       device_(device) {}
 
@@ -36,13 +37,22 @@ void SubIso::Run() {
   auto t0 = std::chrono::steady_clock::now();
   LoadData();
   auto t1 = std::chrono::steady_clock::now();
+  void* model = nullptr;
+  if (order_ == MG_ORDER_LEARNED && !model_path_.empty())
+    Check(mg_order_model_load(model_path_.c_str(), device_, &model));
   void* dg = nullptr;
-  Check(mg_graph_upload(&g_, device_, &dg));
+  int rc = mg_graph_upload(&g_, device_, &dg);
+  if (rc != MG_OK) {
+    const std::string msg = mg_last_error();
+    if (model) mg_order_model_free(model);
+    throw Error(rc, msg);
+  }
   mg_opts o;
   mg_opts_default(&o);
   o.order = order_;
+  o.model = model;
   mg_stats st;
-  int rc = mg_subiso_count_ex(dg, &p_, &o, &count_, &st);
+  rc = mg_subiso_count_ex(dg, &p_, &o, &count_, &st);
   if (rc == MG_OK && mode_ == "emit") {
     k_ = p_.n;
     rows_.assign(count_ * k_, 0);
@@ -50,8 +60,10 @@ void SubIso::Run() {
     rc = mg_subiso_emit(dg, &p_, &o, rows_.data(), count_, &n);
   }
   auto t2 = std::chrono::steady_clock::now();
+  const std::string msg = rc == MG_OK ? "" : mg_last_error();
   mg_graph_free(dg);
-  Check(rc);
+  if (model) mg_order_model_free(model);
+  if (rc != MG_OK) throw Error(rc, msg);
   match_ms_ = st.device_ms;
   std::cout << "[SubIso] LoadData() elapsed: "
             << std::chrono::duration<double>(t1 - t0).count() << " s" << std::endl;
@@ -70,6 +82,63 @@ void SubIso::Write() const {
     for (uint32_t c = 0; c < k_; ++c) f << (c ? "," : "") << rows_[r * k_ + c];
     f << "\n";
   }
+}
+
+BatchSubIso::BatchSubIso(const std::vector<std::string>& pattern_paths,
+                         const std::string& data_graph_path, const std::string& output_path,
+                         int order, const std::string& model_path, int device)
+    : pattern_paths_(pattern_paths),
+      data_graph_path_(data_graph_path),
+      output_path_(output_path),
+      model_path_(model_path),
+      order_(order),
+      device_(device) {}
+
+BatchSubIso::~BatchSubIso() {
+  for (void* o : p_owner_)
+    if (o) mg_csr_dir_close(o);
+  if (g_owner_) mg_csr_dir_close(g_owner_);
+}
+
+void BatchSubIso::Run() {
+  if (pattern_paths_.empty()) throw Error(MG_E_ARG, "no pattern paths in the batch");
+  p_.assign(pattern_paths_.size(), mg_csr_view{});
+  p_owner_.assign(pattern_paths_.size(), nullptr);
+  for (size_t i = 0; i < pattern_paths_.size(); ++i)
+    Check(mg_csr_dir_open(pattern_paths_[i].c_str(), &p_[i], &p_owner_[i]));
+  Check(mg_csr_dir_open(data_graph_path_.c_str(), &g_, &g_owner_));
+  void* model = nullptr;
+  if (order_ == MG_ORDER_LEARNED && !model_path_.empty())
+    Check(mg_order_model_load(model_path_.c_str(), device_, &model));
+  void* dg = nullptr;
+  int rc = mg_graph_upload(&g_, device_, &dg);
+  if (rc == MG_OK) {
+    mg_opts o;
+    mg_opts_default(&o);
+    o.order = order_;
+    o.model = model;
+    std::vector<const mg_csr_view*> qs;
+    for (auto& v : p_) qs.push_back(&v);
+    counts_.assign(qs.size(), 0);
+    mg_stats st;
+    rc = mg_subiso_batch_count_ex(dg, qs.data(), uint32_t(qs.size()), &o, counts_.data(), &st);
+    if (rc == MG_OK)
+      std::cout << "[BatchSubIso] " << qs.size() << " patterns, device " << st.device_ms
+                << " ms, " << st.launches << " launches" << std::endl;
+  }
+  const std::string msg = rc == MG_OK ? "" : mg_last_error();
+  if (dg) mg_graph_free(dg);
+  if (model) mg_order_model_free(model);
+  if (rc != MG_OK) throw Error(rc, msg);
+  std::ostream* os = &std::cout;
+  std::ofstream f;
+  if (!output_path_.empty()) {
+    f.open(output_path_);
+    if (!f) throw Error(MG_E_IO, "cannot write " + output_path_);
+    os = &f;
+  }
+  for (size_t i = 0; i < counts_.size(); ++i)
+    *os << pattern_paths_[i] << " " << counts_[i] << "\n";
 }
 
 int GARMatch::Run(const uint32_t* g_v_id, const int32_t* g_v_label_idx, int g_n_vertices,
@@ -107,6 +176,12 @@ void GARMatch::Run() {
 void MatrixGraph::Run(TaskType type, SubIso* task) {
   (void)scheduler_;
   if (type != kSubIso) throw Error(MG_E_ARG, "a SubIso task needs kSubIso");
+  task->Run();
+}
+
+void MatrixGraph::Run(TaskType type, BatchSubIso* task) {
+  (void)scheduler_;
+  if (type != kSubIso) throw Error(MG_E_ARG, "a BatchSubIso task needs kSubIso");
   task->Run();
 }
 

@@ -41,7 +41,8 @@ class SubIso {
  public:
   SubIso(const std::string& pattern_path, const std::string& data_graph_path,
          const std::string& data_graph_edgelist_path, const std::string& output_path,
-         const std::string& mode = "count", int order = MG_ORDER_REFERENCE, int device = 0);
+         const std::string& mode = "count", int order = MG_ORDER_REFERENCE, int device = 0,
+         const std::string& model_path = "");
   ~SubIso();
   void Run();
 
@@ -54,7 +55,7 @@ class SubIso {
   void Write() const;
 
   std::string pattern_path_, data_graph_path_, data_graph_edgelist_path_, output_path_;
-  std::string mode_;
+  std::string mode_, model_path_;
   int order_, device_;
   mg_csr_view p_{}, g_{};
   void* p_owner_ = nullptr;
@@ -63,6 +64,30 @@ class SubIso {
   uint32_t k_ = 0;
   std::vector<uint32_t> rows_;
   double match_ms_ = 0;
+};
+
+// Many patterns against one resident data graph in one batched call
+// (mg_subiso_batch_count_ex, learned orders planned in one inference
+// launch).  No counterpart in the reference, whose CLI takes one pattern.
+class BatchSubIso {
+ public:
+  BatchSubIso(const std::vector<std::string>& pattern_paths, const std::string& data_graph_path,
+              const std::string& output_path, int order = MG_ORDER_REFERENCE,
+              const std::string& model_path = "", int device = 0);
+  ~BatchSubIso();
+  void Run();
+
+  const std::vector<uint64_t>& counts() const { return counts_; }
+
+ private:
+  std::vector<std::string> pattern_paths_;
+  std::string data_graph_path_, output_path_, model_path_;
+  int order_, device_;
+  std::vector<mg_csr_view> p_;
+  std::vector<void*> p_owner_;
+  mg_csr_view g_{};
+  void* g_owner_ = nullptr;
+  std::vector<uint64_t> counts_;
 };
 
 // GAR match over serialized arrays: the reference's GARGraphArrays,
@@ -138,6 +163,7 @@ class MatrixGraph {
  public:
   explicit MatrixGraph(SchedulerType scheduler = kCHBL) : scheduler_(scheduler) {}
   void Run(TaskType type, SubIso* task);
+  void Run(TaskType type, BatchSubIso* task);
   void Run(TaskType type, GARMatch* task);
 
  private:

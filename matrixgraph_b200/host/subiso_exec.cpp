@@ -1,12 +1,17 @@
 // subiso_exec: the reference's subiso CLI (apps/subiso.cu:16-97) over the
 // C-ABI.  Flags: -p <pattern dir/> -g <graph dir/> [-e <edge list, unused>]
 // [-o <output>] [-scheduler CHBL|EvenSplit|RoundRobin] plus
-// [-mode count|emit] [-order reference|strong] [-device N].
+// [-mode count|emit] [-order reference|heuristic|strong|learned]
+// [-model <order model dir/>] [-batch <file of pattern dirs, one per line>]
+// [-device N].  With -batch, -p is not needed and every pattern is counted
+// in one batched call; -o receives "pattern count" lines.
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <iostream>
 #include <map>
 #include <string>
+#include <vector>
 
 #include "matrixgraph.h"
 
@@ -23,7 +28,8 @@ static SchedulerType Scheduler2Enum(const std::string& s) {
 int main(int argc, char** argv) {
   std::map<std::string, std::string> flags = {
       {"p", ""}, {"g", ""}, {"e", ""}, {"o", ""}, {"scheduler", "CHBL"},
-      {"mode", "count"}, {"order", "reference"}, {"device", "0"}};
+      {"mode", "count"}, {"order", "reference"}, {"device", "0"}, {"batch", ""},
+      {"model", ""}};
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i];
     while (!a.empty() && a[0] == '-') a = a.substr(1);
@@ -42,7 +48,35 @@ int main(int argc, char** argv) {
     flags[a] = v;
   }
   bool ok = true;
-  if (flags["p"].empty()) {
+  static const std::map<std::string, int> kOrders = {{"reference", MG_ORDER_REFERENCE},
+                                                     {"heuristic", MG_ORDER_REFERENCE},
+                                                     {"strong", MG_ORDER_STRONG},
+                                                     {"learned", MG_ORDER_LEARNED}};
+  if (!kOrders.count(flags["order"])) {
+    std::cerr << "Error: unknown order " << flags["order"] << std::endl;
+    ok = false;
+  }
+  if (flags["order"] == "learned" && flags["model"].empty()) {
+    std::cerr << "Error: -order learned needs -model <order model dir/>" << std::endl;
+    ok = false;
+  }
+  std::vector<std::string> batch;
+  if (!flags["batch"].empty()) {
+    std::ifstream f(flags["batch"]);
+    if (!f) {
+      std::cerr << "Error: cannot read the batch list " << flags["batch"] << std::endl;
+      return EXIT_FAILURE;
+    }
+    for (std::string line; std::getline(f, line);) {
+      while (!line.empty() && (line.back() == '\r' || line.back() == ' ')) line.pop_back();
+      if (!line.empty() && line[0] != '#') batch.push_back(line);
+    }
+    if (batch.empty()) {
+      std::cerr << "Error: the batch list " << flags["batch"] << " names no pattern" << std::endl;
+      ok = false;
+    }
+  }
+  if (flags["p"].empty() && batch.empty()) {
     std::cerr << "Error: Pattern graph path (-p) is required" << std::endl;
     ok = false;
   }
@@ -53,7 +87,8 @@ int main(int argc, char** argv) {
   if (!ok) {
     std::cerr << "Usage: " << argv[0] << " -p <pattern_path/> -g <graph_path/> [-e <edge_list>]"
               << " [-o <output_path>] [-scheduler CHBL] [-mode count|emit]"
-              << " [-order reference|strong] [-device N]" << std::endl;
+              << " [-order reference|strong|learned] [-model <dir/>] [-batch <list>]"
+              << " [-device N]" << std::endl;
     return EXIT_FAILURE;
   }
   std::cout << "\n=== SubIso Configuration ===\nPattern Graph: " << flags["p"]
@@ -62,10 +97,17 @@ int main(int argc, char** argv) {
             << "\n==========================\n" << std::endl;
   try {
     MatrixGraph system(Scheduler2Enum(flags["scheduler"]));
-    int order = flags["order"] == "strong" ? MG_ORDER_STRONG : MG_ORDER_REFERENCE;
-    SubIso task(flags["p"], flags["g"], flags["e"], flags["o"], flags["mode"], order,
-                std::atoi(flags["device"].c_str()));
-    system.Run(matrixgraph::kSubIso, &task);
+    const int order = kOrders.at(flags["order"]);
+    const int device = std::atoi(flags["device"].c_str());
+    if (!batch.empty()) {
+      matrixgraph::BatchSubIso task(batch, flags["g"], flags["o"], order, flags["model"],
+                                    device);
+      system.Run(matrixgraph::kSubIso, &task);
+    } else {
+      SubIso task(flags["p"], flags["g"], flags["e"], flags["o"], flags["mode"], order, device,
+                  flags["model"]);
+      system.Run(matrixgraph::kSubIso, &task);
+    }
   } catch (const std::exception& e) {
     std::cerr << "Error: " << e.what() << std::endl;
     return EXIT_FAILURE;
