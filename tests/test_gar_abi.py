@@ -162,3 +162,21 @@ def test_subdivided_instance_against_oracle(seed):
         assert res.matched_v_ids.tolist() == orc.matched_v_ids
         assert res.row_count.tolist() == orc.row_count
         assert res.row_pivot_id.tolist() == orc.row_pivot_id
+
+
+def test_pattern_limits_before_any_device_work():
+    from oracle.gar import GarGraph, GarPattern
+    # every vertex label 0, edges of labels 0 and 1 in both directions along a path
+    n = 20
+    src = list(range(n - 1)) + list(range(1, n))
+    dst = list(range(1, n)) + list(range(n - 1))
+    g = GarGraph(v_id=None, v_label=[0] * n, e_src=src * 2, e_dst=dst * 2,
+                 e_label=[0] * len(src) + [1] * len(src), n_vertices=n)
+    # 17 pattern nodes on a path: beyond 16
+    p = GarPattern([0] * 17, list(range(16)), list(range(1, 17)), [0] * 16, 17)
+    rc, r = gar_match(*_lib_inputs(g, p), 10, 10, raw=True)
+    assert rc == L.MG_E_LIMIT and r.num_conditions == 1
+    # 9 nodes and 8 distinct edges over two edge labels: 17 subdivided vertices
+    p = GarPattern([0] * 9, list(range(8)), list(range(1, 9)), [i % 2 for i in range(8)], 9)
+    rc, r = gar_match(*_lib_inputs(g, p), 10, 10, raw=True)
+    assert rc == L.MG_E_LIMIT and b"distinct edges" in L.lib.mg_last_error()
