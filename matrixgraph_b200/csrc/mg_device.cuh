@@ -83,6 +83,7 @@ struct Workspace;  // enumeration scratch (mg_enum.cu)
 // Host object behind the opaque dgraph handle.
 struct DevGraph {
   int device = 0;
+  unsigned sms = 1;  // multiprocessors of the device (grid sizing)
   cudaStream_t stream = nullptr;
   GraphDev g{};
   mg_graph_info info{};

@@ -1007,7 +1007,7 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
   R[0] = nq;
   int lvl = 0;
   bool need_work = true;
-  const unsigned sms = 148;
+  const unsigned sms = dg->sms;
   uint64_t elements = 0;
 
   // Pendant tails counted in closed form (count mode): tail-key table and
@@ -1592,92 +1592,19 @@ uint64_t noalloc_carve(unsigned char* base, uint64_t cap, uint32_t k, NoallocLay
   return off;
 }
 
-// Query normalisation into fixed-size storage (no heap): labels, edge masks
-// and the directed edges in CSR order.
-int noalloc_query(const mg_csr_view* q, QueryGraph* Q, uint32_t (*edges)[2], uint32_t* ne) {
-  int rc = validate_csr_view(q);
-  if (rc) return rc;
-  if (q->n == 0) return set_error(MG_E_ARG, "empty query");
-  if (q->n > MG_MAX_QUERY_VERTICES)
-    return set_error(MG_E_LIMIT, "query has %u vertices; at most %d supported", q->n,
-                     MG_MAX_QUERY_VERTICES);
-  Q->k = q->n;
-  *ne = 0;
-  for (uint32_t i = 0; i < q->n; ++i) {
-    Q->label_raw[i] = q->labels[i];
-    Q->out_mask[i] = Q->in_mask[i] = 0;
-    for (uint32_t j = 0; j < i; ++j)
-      if (q->globalid[j] == q->globalid[i])
-        return set_error(MG_E_FORMAT, "query globalid %u repeated", q->globalid[i]);
-  }
-  for (uint32_t u = 0; u < q->n; ++u)
-    for (uint32_t e = q->out_off[u]; e < q->out_off[u + 1]; ++e) {
-      uint32_t w = FULL;
-      for (uint32_t x = 0; x < q->n; ++x)
-        if (q->globalid[x] == q->out_edges[e]) w = x;
-      if (w == FULL)
-        return set_error(MG_E_FORMAT, "query out-edge to unknown vertex %u", q->out_edges[e]);
-      if (!((Q->out_mask[u] >> w) & 1u)) {
-        edges[*ne][0] = u;
-        edges[*ne][1] = w;
-        ++*ne;
-      }
-      Q->out_mask[u] |= 1u << w;
-      Q->in_mask[w] |= 1u << u;
-    }
-  return MG_OK;
-}
-
-// The reference vertex-introduction order over a fixed edge array (same rule
-// as order_reference).
-void noalloc_order_reference(uint32_t k, const uint32_t (*edges)[2], uint32_t ne,
-                             uint32_t* order) {
-  uint32_t placed = 0, n = 0;
-  auto place = [&](uint32_t v) {
-    if (!((placed >> v) & 1u)) {
-      placed |= 1u << v;
-      order[n++] = v;
-    }
-  };
-  if (ne) {
-    place(edges[0][0]);
-    place(edges[0][1]);
-  }
-  while (n < k) {
-    bool changed = true;
-    while (changed) {
-      changed = false;
-      for (uint32_t e = 0; e < ne; ++e) {
-        const bool a = (placed >> edges[e][0]) & 1u, b = (placed >> edges[e][1]) & 1u;
-        if (a && !b) {
-          place(edges[e][1]);
-          changed = true;
-        } else if (b && !a) {
-          place(edges[e][0]);
-          changed = true;
-        }
-      }
-    }
-    for (uint32_t v = 0; v < k && n < k; ++v)
-      if (!((placed >> v) & 1u)) {
-        place(v);
-        break;
-      }
-  }
-}
-
 int noalloc_count(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint64_t* count) {
   mg_opts o;
   mg_opts_default(&o);
   if (opts) o = *opts;
+  // Every argument is checked before any work is queued on the shared array.
+  if (o.root_end && o.root_begin > o.root_end)
+    return set_error(MG_E_ARG, "root_begin > root_end");
   QueryGraph Q;
-  uint32_t edges[MAXK * MAXK][2];
-  uint32_t ne = 0;
-  int rc = noalloc_query(q, &Q, edges, &ne);
+  int rc = normalise_query(q, &Q);  // the allocating entry points' normaliser
   if (rc) return rc;
   uint32_t order[MAXK];
   if (o.order == MG_ORDER_REFERENCE) {
-    noalloc_order_reference(Q.k, edges, ne, order);
+    order_reference(Q, order);
   } else if (o.order == MG_ORDER_STRONG) {
     order_strong(Q, dg->stats, order);
   } else if (o.order == MG_ORDER_GIVEN) {
@@ -1739,9 +1666,9 @@ int noalloc_count(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint6
   a.count_mode = 1;
   a.filters = o.filters & MG_FILTER_ALL;
   a.nq = 1;
+  a.grab = o.grab;
   a.tile_row = L.tile_row;
   if (o.root_end) {
-    if (o.root_begin > o.root_end) return set_error(MG_E_ARG, "root_begin > root_end");
     a.root_begin = o.root_begin;
     a.root_end = o.root_end;
   }
@@ -1753,8 +1680,8 @@ int noalloc_count(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint6
     for (uint32_t j = 0; j < l; ++j) t.col[j] = L.col[l][j];
     return t;
   };
-  const unsigned sms = 148;
-  uint64_t T[MAXK] = {}, cur[MAXK] = {}, host_u64 = 0;
+  const unsigned sms = dg->sms;
+  uint64_t T[MAXK] = {}, cur[MAXK] = {}, host_u64 = 0, elements = 0;
   uint32_t R[MAXK] = {};
   R[0] = 1;
   int lvl = 0;
@@ -1782,6 +1709,12 @@ int noalloc_count(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint6
     if (cur[lvl] < T[lvl]) {
       const uint64_t t0 = cur[lvl];
       const uint64_t t1 = writes[lvl] ? std::min(T[lvl], t0 + cap) : T[lvl];
+      elements += t1 - t0;
+      if (o.max_elements && elements > o.max_elements) {
+        cudaStreamSynchronize(st);  // nothing of this call stays queued on the array
+        return set_error(MG_E_LIMIT, "work budget of %llu candidate elements exceeded",
+                         (unsigned long long)o.max_elements);
+      }
       a.out = writes[lvl] ? tab(lvl + 1) : TabPtrs{};
       a.out_cap = writes[lvl] ? cap : 0;
       MG_CK(cudaMemsetAsync(L.ctr + C_OUT, 0, 8, st));

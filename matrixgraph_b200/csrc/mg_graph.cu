@@ -242,7 +242,7 @@ bool arrays_equal(const uint32_t* a, const uint32_t* b, uint64_t words) {
   return true;
 }
 
-inline unsigned grid_for(uint64_t items, unsigned block, unsigned cap = 148 * 32) {
+inline unsigned grid_for(uint64_t items, unsigned block, unsigned cap) {
   uint64_t g = (items + block - 1) / block;
   return unsigned(std::max<uint64_t>(1, std::min<uint64_t>(g, cap)));
 }
@@ -260,10 +260,10 @@ static int build_direction(DevGraph* dg, int d, const uint32_t* h_off, const uin
   MG_CK(cudaMallocAsync((void**)&adj, std::max<uint64_t>(1, m) * 4ull, st));
   MG_CK(cudaMemcpyAsync(off, h_off, (uint64_t(n) + 1) * 4, cudaMemcpyHostToDevice, st));
   if (m) MG_CK(cudaMemcpyAsync(adj, h_adj, uint64_t(m) * 4, cudaMemcpyHostToDevice, st));
-  if (d_g2l && m) k_map_edges<<<grid_for(m, 256), 256, 0, st>>>(adj, m, d_g2l, max_vid, d_err);
+  if (d_g2l && m) k_map_edges<<<grid_for(m, 256, dg->sms * 32), 256, 0, st>>>(adj, m, d_g2l, max_vid, d_err);
   uint32_t* d_flags = d_err + 1;
   MG_CK(cudaMemsetAsync(d_flags, 0, 4, st));
-  k_check_lists<<<grid_for(uint64_t(n) * 32, 256), 256, 0, st>>>(off, adj, n, d_flags);
+  k_check_lists<<<grid_for(uint64_t(n) * 32, 256, dg->sms * 32), 256, 0, st>>>(off, adj, n, d_flags);
   uint32_t flags = 0;
   MG_CK(cudaMemcpyAsync(&flags, d_flags, 4, cudaMemcpyDeviceToHost, st));
   MG_CK(cudaStreamSynchronize(st));
@@ -288,14 +288,14 @@ static int build_direction(DevGraph* dg, int d, const uint32_t* h_off, const uin
     uint32_t *newdeg = nullptr, *newoff = nullptr;
     MG_CK(cudaMallocAsync((void**)&newdeg, (uint64_t(n) + 1) * 4, st));
     MG_CK(cudaMallocAsync((void**)&newoff, (uint64_t(n) + 1) * 4, st));
-    k_count_unique<<<grid_for(uint64_t(n) * 32, 256), 256, 0, st>>>(off, sorted, n, newdeg);
+    k_count_unique<<<grid_for(uint64_t(n) * 32, 256, dg->sms * 32), 256, 0, st>>>(off, sorted, n, newdeg);
     tmp_bytes = 0;
     MG_CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, newdeg, newoff, n + 1, st));
     MG_CK(cudaMallocAsync(&tmp, std::max<size_t>(16, tmp_bytes), st));
     k_set_u32<<<1, 1, 0, st>>>(newdeg, n, 0);
     MG_CK(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, newdeg, newoff, n + 1, st));
     cudaFreeAsync(tmp, st);
-    k_compact_unique<<<grid_for(uint64_t(n) * 32, 256), 256, 0, st>>>(off, sorted, n, newoff, adj);
+    k_compact_unique<<<grid_for(uint64_t(n) * 32, 256, dg->sms * 32), 256, 0, st>>>(off, sorted, n, newoff, adj);
     MG_CK(cudaMemcpyAsync(&mm, newoff + n, 4, cudaMemcpyDeviceToHost, st));
     cudaFreeAsync(sorted, st);
     cudaFreeAsync(newdeg, st);
@@ -311,7 +311,7 @@ static int build_direction(DevGraph* dg, int d, const uint32_t* h_off, const uin
   if ((rc = dev_alloc(dg, (void**)&deg, uint64_t(n) * 4))) return rc;
   const unsigned block = 256;
   const size_t smem = size_t(block / 32) * L * 4;
-  k_partition_labels<<<grid_for(uint64_t(n) * 32, block, 148 * 16), block, smem, st>>>(
+  k_partition_labels<<<grid_for(uint64_t(n) * 32, block, dg->sms * 16), block, smem, st>>>(
       off, adj, n, d_label, L, W, loff, adjL, nlb, deg, const_cast<uint32_t*>(dg->g.selfbits));
   k_set_u32<<<1, 1, 0, st>>>(loff, uint64_t(n) * L, mm);
   MG_CK(cudaGetLastError());
@@ -336,6 +336,9 @@ static int upload(const mg_csr_view* v, int device, DevGraph* dg) {
     return set_error(MG_E_ARG, "device %d not present (%d devices)", device, ndev);
   MG_CK(cudaSetDevice(device));
   dg->device = device;
+  int sms = 0;
+  MG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  dg->sms = unsigned(std::max(sms, 1));
   MG_CK(cudaStreamCreateWithFlags(&dg->stream, cudaStreamNonBlocking));
   cudaStream_t st = dg->stream;
   const uint32_t n = v->n;
@@ -400,7 +403,7 @@ static int upload(const mg_csr_view* v, int device, DevGraph* dg) {
   if (!ident) {
     MG_CK(cudaMallocAsync((void**)&d_g2l, (uint64_t(v->max_vid) + 1) * 4, st));
     MG_CK(cudaMemsetAsync(d_g2l, 0xFF, (uint64_t(v->max_vid) + 1) * 4, st));
-    k_build_g2l<<<grid_for(n, 256), 256, 0, st>>>(d_gid, n, d_g2l, v->max_vid, d_err);
+    k_build_g2l<<<grid_for(n, 256, dg->sms * 32), 256, 0, st>>>(d_gid, n, d_g2l, v->max_vid, d_err);
   }
   const bool sym = v->m_in == v->m_out && arrays_equal(v->in_off, v->out_off, uint64_t(n) + 1) &&
                    arrays_equal(v->in_edges, v->out_edges, v->m_out);
@@ -449,7 +452,7 @@ int ensure_full_stats(DevGraph* dg) {
   MG_CK(cudaMemsetAsync(dhist, 0, L * 33 * 8ull, st));
   MG_CK(cudaMemsetAsync(dpair, 0, uint64_t(L) * L * 8, st));
   MG_CK(cudaMemsetAsync(dmax, 0, L * 4ull, st));
-  k_label_stats<<<grid_for(n, 256), 256, 0, st>>>(dg->g.loff[0], dg->g.label, n, L, dsum, dmax,
+  k_label_stats<<<grid_for(n, 256, dg->sms * 32), 256, 0, st>>>(dg->g.loff[0], dg->g.label, n, L, dsum, dmax,
                                                   dhist, dpair);
   std::vector<unsigned long long> hsum(L), hhist(L * 33), hpair(uint64_t(L) * L);
   std::vector<unsigned int> hmax(L);

@@ -73,13 +73,17 @@ struct RngStream {
 };
 
 // ---- normalised query -------------------------------------------------------
-// Local ids 0..k-1 (CSR row order), edge sets as bit masks, raw labels.
+// Local ids 0..k-1 (CSR row order), edge sets as bit masks, raw labels, and
+// the distinct directed edges in CSR order.  Fixed-size storage: normalising
+// a query touches no heap, so allocation-free entry points share it.
 struct QueryGraph {
   uint32_t k = 0;
   uint32_t label_raw[MG_MAX_QUERY_VERTICES];
   uint32_t out_mask[MG_MAX_QUERY_VERTICES];  // bit w set: edge u -> w
   uint32_t in_mask[MG_MAX_QUERY_VERTICES];   // bit w set: edge w -> u
-  std::vector<std::pair<uint32_t, uint32_t>> edges_csr_order;  // directed
+  uint32_t n_edges = 0;
+  uint8_t edge_u[MG_MAX_QUERY_VERTICES * MG_MAX_QUERY_VERTICES];
+  uint8_t edge_w[MG_MAX_QUERY_VERTICES * MG_MAX_QUERY_VERTICES];
 };
 int normalise_query(const mg_csr_view* q, QueryGraph* out);
 

@@ -67,6 +67,7 @@ struct Sample {
 
 struct OrderModel {
   int device = 0;
+  unsigned sms = 1;  // multiprocessors of the device
   cudaStream_t stream = nullptr;
   float* params = nullptr;   // NPARAM
   float* grad = nullptr;
@@ -313,6 +314,9 @@ const size_t kTrainSmem = size_t(NPARAM) * 4;
 int model_init(OrderModel* M, int device) {
   M->device = device;
   MG_CK(cudaSetDevice(device));
+  int sms = 0;
+  MG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  M->sms = unsigned(std::max(sms, 1));
   MG_CK(cudaStreamCreateWithFlags(&M->stream, cudaStreamNonBlocking));
   MG_CK(cudaMalloc((void**)&M->params, NPARAM * 4));
   MG_CK(cudaMalloc((void**)&M->grad, NPARAM * 4));
@@ -404,7 +408,7 @@ int infer(OrderModel* M, const std::vector<QFeat>& qf, const std::vector<Sample>
   MG_CK(cudaMallocAsync((void**)&dout, smp.size() * 4, st));
   MG_CK(cudaMemcpyAsync(dq, qf.data(), qf.size() * sizeof(QFeat), cudaMemcpyHostToDevice, st));
   MG_CK(cudaMemcpyAsync(ds, smp.data(), smp.size() * sizeof(Sample), cudaMemcpyHostToDevice, st));
-  const unsigned blocks = unsigned(std::min<size_t>(smp.size(), 148 * 32));
+  const unsigned blocks = unsigned(std::min<size_t>(smp.size(), size_t(M->sms) * 32));
   k_mpnn_infer_bf16<<<blocks, MH, 0, st>>>(M->params_bf16, dq, ds, uint32_t(smp.size()), dout);
   MG_CK(cudaMemcpyAsync(out.data(), dout, smp.size() * 4, cudaMemcpyDeviceToHost, st));
   cudaFreeAsync(dq, st);
@@ -576,7 +580,7 @@ static int gather(DevGraph* dg, const mg_csr_view* const* qs, uint32_t nq,
 
 static int train_pass(OrderModel* M, const QFeat* dq, const Sample* ds, uint32_t ns, float scale,
                       bool backward, float* dloss, float* dout) {
-  const unsigned blocks = std::max(1u, std::min<unsigned>(ns, 148 * 2));
+  const unsigned blocks = std::max(1u, std::min<unsigned>(ns, M->sms * 2));
   if (backward) MG_CK(cudaMemsetAsync(M->grad, 0, NPARAM * 4, M->stream));
   k_mpnn_train<<<blocks, MH, kTrainSmem, M->stream>>>(M->params, dq, ds, ns, scale,
                                                        backward ? 1 : 0, M->grad, dloss, dout);

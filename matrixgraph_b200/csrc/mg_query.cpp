@@ -1,7 +1,6 @@
 // Query normalisation and matching orders.
 #include <algorithm>
 #include <cstring>
-#include <unordered_map>
 
 #include "mg_internal.h"
 
@@ -20,22 +19,29 @@ int normalise_query(const mg_csr_view* q, QueryGraph* out) {
                      MG_MAX_QUERY_VERTICES);
   QueryGraph& Q = *out;
   Q.k = q->n;
-  std::unordered_map<uint32_t, uint32_t> g2l;
+  // Global -> local id by a linear scan (k <= 16): no heap.
+  auto local = [&](uint32_t gid) -> uint32_t {
+    for (uint32_t x = 0; x < q->n; ++x)
+      if (q->globalid[x] == gid) return x;
+    return UINT32_MAX;
+  };
   for (uint32_t i = 0; i < q->n; ++i) {
-    if (g2l.count(q->globalid[i]))
+    if (local(q->globalid[i]) != i)
       return set_error(MG_E_FORMAT, "query globalid %u repeated", q->globalid[i]);
-    g2l[q->globalid[i]] = i;
     Q.label_raw[i] = q->labels[i];
     Q.out_mask[i] = Q.in_mask[i] = 0;
   }
-  Q.edges_csr_order.clear();
+  Q.n_edges = 0;
   for (uint32_t u = 0; u < q->n; ++u) {
     for (uint32_t e = q->out_off[u]; e < q->out_off[u + 1]; ++e) {
-      auto it = g2l.find(q->out_edges[e]);
-      if (it == g2l.end())
+      const uint32_t w = local(q->out_edges[e]);
+      if (w == UINT32_MAX)
         return set_error(MG_E_FORMAT, "query out-edge to unknown vertex %u", q->out_edges[e]);
-      uint32_t w = it->second;
-      if (!(Q.out_mask[u] >> w & 1)) Q.edges_csr_order.emplace_back(u, w);
+      if (!(Q.out_mask[u] >> w & 1)) {
+        Q.edge_u[Q.n_edges] = uint8_t(u);
+        Q.edge_w[Q.n_edges] = uint8_t(w);
+        ++Q.n_edges;
+      }
       Q.out_mask[u] |= 1u << w;
       Q.in_mask[w] |= 1u << u;
     }
@@ -46,10 +52,10 @@ int normalise_query(const mg_csr_view* q, QueryGraph* out) {
     uint32_t in_mask[MG_MAX_QUERY_VERTICES] = {0};
     for (uint32_t u = 0; u < q->n; ++u)
       for (uint32_t e = q->in_off[u]; e < q->in_off[u + 1]; ++e) {
-        auto it = g2l.find(q->in_edges[e]);
-        if (it == g2l.end())
+        const uint32_t w = local(q->in_edges[e]);
+        if (w == UINT32_MAX)
           return set_error(MG_E_FORMAT, "query in-edge from unknown vertex %u", q->in_edges[e]);
-        in_mask[u] |= 1u << it->second;
+        in_mask[u] |= 1u << w;
       }
     for (uint32_t u = 0; u < q->n; ++u)
       if (in_mask[u] != Q.in_mask[u])
@@ -88,22 +94,21 @@ void order_reference(const QueryGraph& q, uint32_t* order) {
       order[n++] = v;
     }
   };
-  const auto& E = q.edges_csr_order;
-  if (!E.empty()) {
-    place(E[0].first);
-    place(E[0].second);
+  if (q.n_edges) {
+    place(q.edge_u[0]);
+    place(q.edge_w[0]);
   }
   while (n < q.k) {
     bool changed = true;
     while (changed) {
       changed = false;
-      for (auto& e : E) {
-        bool a = placed >> e.first & 1, b = placed >> e.second & 1;
+      for (uint32_t e = 0; e < q.n_edges; ++e) {
+        bool a = placed >> q.edge_u[e] & 1, b = placed >> q.edge_w[e] & 1;
         if (a && !b) {
-          place(e.second);
+          place(q.edge_w[e]);
           changed = true;
         } else if (b && !a) {
-          place(e.first);
+          place(q.edge_u[e]);
           changed = true;
         }
       }

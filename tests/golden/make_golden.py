@@ -1,9 +1,10 @@
 """Generates the committed golden fixtures under tests/golden/.
 
 Run from the repository root in a container where the reference project is
-mounted at /root/reference (it is read here, never at test time):
+checked out (read here, never at test time), given as the argument or as
+MG_REFERENCE_DIR:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <reference checkout>
 
 Fixtures:
   toy_graph/            the reference's only data fixture
@@ -33,7 +34,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference"
+# The reference checkout to read fixtures from: first argument or
+# MG_REFERENCE_DIR (required; there is no default location).
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MG_REFERENCE_DIR", "")
+if __name__ == "__main__" and not os.path.isdir(os.path.join(REF, "core")):
+    sys.exit("usage: make_golden.py <reference checkout> (or set MG_REFERENCE_DIR)")
 sys.path.insert(0, ROOT)
 
 
