@@ -96,9 +96,13 @@ typedef struct mg_opts {
   uint32_t grab;             /* expand tiles (256 candidates each) a block
                                 takes from the device work queue at a time;
                                 0 = auto                                     */
-  uint32_t merge_min;        /* reserved, 0                                  */
-  uint32_t spin_limit;       /* iteration cap of device waits; 0 = default   */
-  uint32_t persistent;       /* 1: one persistent launch drives all levels  */
+  uint32_t root_step;        /* level-0 candidates are the bucket positions
+                                root_begin, root_begin + root_step, ... below
+                                root_end (0 or 1: every position).  A stride
+                                equal to the rank count with root_begin =
+                                rank spreads the hub roots evenly over ranks */
+  uint32_t _reserved0;       /* must be 0                                    */
+  uint32_t _reserved1;       /* must be 0                                    */
   uint64_t mem_budget_bytes; /* cap on enumeration scratch; 0 = auto        */
   uint64_t root_begin;       /* level-0 candidates [root_begin, root_end) of  */
   uint64_t root_end;         /* the first position's label bucket; 0,0 = all  */

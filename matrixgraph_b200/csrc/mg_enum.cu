@@ -187,6 +187,7 @@ struct StepArgs {
   uint32_t* emit_col[MAXK];
   uint64_t emit_cap;
   uint64_t root_begin, root_end;  // level-0 candidate range (root_end 0: all)
+  uint32_t root_step;             // level-0 stride inside the range (>= 1)
   const uint32_t* tile_row;        // first row of each tile of [t0, t1)
   // Pendant tails counted in closed form (tail_on): memo table of aggregates.
   uint32_t grab;   // expand tiles taken per work-queue grab
@@ -475,7 +476,7 @@ __global__ void __launch_bounds__(256) k_work(StepArgs a) {
         const uint64_t rb = a.root_begin < best ? a.root_begin : uint64_t(best);
         const uint64_t re = a.root_end < best ? a.root_end : uint64_t(best);
         bs += uint32_t(rb);
-        best = re > rb ? uint32_t(re - rb) : 0u;
+        best = re > rb ? uint32_t((re - rb + a.root_step - 1) / a.root_step) : 0u;
       }
       ch = chc = (unsigned long long)best * (12ull + 4ull * g.W);
     } else {
@@ -668,7 +669,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
         const uint32_t lab = P.label[i];
         uint32_t ddir = 0;
         if (ci == DCI_BUCKET) {
-          x = __ldg(g.bucket_vid + ds + e);
+          x = __ldg(g.bucket_vid + ds + (i == 0 ? uint64_t(e) * a.root_step : uint64_t(e)));
         } else {
           ddir = P.cons[i][ci] >> 8;
           x = __ldg(g.adj[ddir] + ds + e);
@@ -992,10 +993,10 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
     for (int j = 0; j < MAXK; ++j) a.emit_col[j] = emit->col[j];
     a.emit_cap = emit->cap;
   }
-  if (o.root_end) {
-    if (o.root_begin > o.root_end) return set_error(MG_E_ARG, "root_begin > root_end");
+  a.root_step = o.root_step > 1 ? o.root_step : 1u;
+  if (o.root_end || a.root_step > 1) {
     a.root_begin = o.root_begin;
-    a.root_end = o.root_end;
+    a.root_end = o.root_end ? o.root_end : ~0ull;
   }
   const bool batch = nq > 1;
   if (batch) {
@@ -1277,6 +1278,14 @@ static mg_opts resolve_opts(const mg_opts* o) {
   return r;
 }
 
+// Checks that do not depend on the query or the graph.
+static int check_opts(const mg_opts& o) {
+  if (o._reserved0 || o._reserved1) return set_error(MG_E_ARG, "reserved option fields must be 0");
+  if (o.root_end && o.root_begin > o.root_end)
+    return set_error(MG_E_ARG, "root_begin > root_end");
+  return MG_OK;
+}
+
 static void fill_stats(mg_stats* st, const PlanDev& P, const RunResult& res, uint64_t count) {
   if (!st) return;
   std::memset(st, 0, sizeof(*st));
@@ -1293,8 +1302,10 @@ static void fill_stats(mg_stats* st, const PlanDev& P, const RunResult& res, uin
 }
 
 static int prepare(DevGraph* dg, const mg_csr_view* q, const mg_opts& o, PlanDev* P) {
+  int rc = check_opts(o);
+  if (rc) return rc;
   QueryGraph Q;
-  int rc = normalise_query(q, &Q);
+  rc = normalise_query(q, &Q);
   if (rc) return rc;
   uint32_t order[MAXK];
   if ((rc = choose_order(dg, Q, o, order))) return rc;
@@ -1597,10 +1608,10 @@ int noalloc_count(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint6
   mg_opts_default(&o);
   if (opts) o = *opts;
   // Every argument is checked before any work is queued on the shared array.
-  if (o.root_end && o.root_begin > o.root_end)
-    return set_error(MG_E_ARG, "root_begin > root_end");
+  int rc = check_opts(o);
+  if (rc) return rc;
   QueryGraph Q;
-  int rc = normalise_query(q, &Q);  // the allocating entry points' normaliser
+  rc = normalise_query(q, &Q);  // the allocating entry points' normaliser
   if (rc) return rc;
   uint32_t order[MAXK];
   if (o.order == MG_ORDER_REFERENCE) {
@@ -1668,9 +1679,10 @@ int noalloc_count(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint6
   a.nq = 1;
   a.grab = o.grab;
   a.tile_row = L.tile_row;
-  if (o.root_end) {
+  a.root_step = o.root_step > 1 ? o.root_step : 1u;
+  if (o.root_end || a.root_step > 1) {
     a.root_begin = o.root_begin;
-    a.root_end = o.root_end;
+    a.root_end = o.root_end ? o.root_end : ~0ull;
   }
   bool writes[MAXK] = {};
   for (uint32_t l = 0; l < k; ++l)

@@ -32,7 +32,7 @@ ORDERS = {"reference": L.MG_ORDER_REFERENCE, "heuristic": L.MG_ORDER_REFERENCE,
 
 
 def make_opts(order="reference", filters=L.MG_FILTER_ALL, chunk_rows=0, given_order=None,
-              model=None, root_range=None, mem_budget_bytes=0, persistent=0,
+              model=None, root_range=None, mem_budget_bytes=0, root_step=0,
               grab=0, no_tail=0, max_elements=0):
     o = L.default_opts()
     o.no_tail = no_tail
@@ -41,7 +41,7 @@ def make_opts(order="reference", filters=L.MG_FILTER_ALL, chunk_rows=0, given_or
     o.filters = filters
     o.chunk_rows = chunk_rows
     o.mem_budget_bytes = mem_budget_bytes
-    o.persistent = persistent
+    o.root_step = root_step
     o.grab = grab
     keep = None
     if given_order is not None:
@@ -174,6 +174,17 @@ def shard_roots(n_roots: int, rank: int, world: int) -> tuple[int, int]:
     base, rem = divmod(n_roots, world)
     begin = rank * base + min(rank, rem)
     return begin, begin + base + (1 if rank < rem else 0)
+
+
+def shard_strided(rank: int, world: int) -> dict:
+    """Count options of one rank's shard: level-0 candidates at bucket
+    positions rank, rank + world, rank + 2*world, ...  A label bucket lists
+    its vertices by id, and generators without id permutation (R-MAT) put
+    the hubs first, so contiguous ranges would hand every hub to rank 0; a
+    stride spreads them evenly.  The shards partition the bucket."""
+    if world <= 1:
+        return {}
+    return {"root_range": (rank, 0), "root_step": world}
 
 
 # ---- reference-shaped task / runtime ------------------------------------------

@@ -21,8 +21,8 @@ def build() -> None:
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(
-        os.path.join(HERE, "oracle.c")):
+if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < max(
+        os.path.getmtime(os.path.join(HERE, f)) for f in ("oracle.c", "gen.c")):
     build()
 
 _lib = C.CDLL(LIB_PATH)
@@ -51,7 +51,19 @@ _lib.orc_graph_info.argtypes = [C.c_void_p, P32, P32, C.POINTER(C.c_int),
 _lib.orc_query_from_arrays.argtypes = [C.c_uint32, P32, P32, P32, P32, C.POINTER(OrcQuery)]
 _lib.orc_order_reference.argtypes = [C.POINTER(OrcQuery), P32]
 _lib.orc_count.argtypes = [C.c_void_p, C.POINTER(OrcQuery), P32, C.c_uint32, C.c_int,
-                           C.c_uint64, C.c_uint64, C.POINTER(OrcResult)]
+                           C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(OrcResult)]
+PP32 = C.POINTER(P32)
+_lib.orc_gen_rmat_csr.argtypes = [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double,
+                                  C.c_uint64, C.c_int, PP32, PP32, C.POINTER(C.c_uint64)]
+_lib.orc_csr_symmetric.argtypes = [C.c_uint32, P32, P32, C.c_uint64, C.c_int, PP32, PP32,
+                                   C.POINTER(C.c_uint64)]
+_lib.orc_gen_labels.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_uint64,
+                                P32]
+_lib.orc_walk_labels.argtypes = [C.c_uint32, P32, P32, P32, C.c_uint32, P32, C.c_uint64,
+                                 C.c_uint64, P32]
+_lib.orc_random_query_shape.argtypes = [C.c_uint32, C.c_double, C.c_uint64, P32]
+_libc = C.CDLL(None)
+_libc.free.argtypes = [C.c_void_p]
 _lib.orc_emit.argtypes = [C.c_void_p, C.POINTER(OrcQuery), P32, C.c_uint32, P32, C.c_uint64,
                           C.POINTER(C.c_uint64)]
 _lib.orc_bucket_size.restype = C.c_uint32
@@ -128,12 +140,16 @@ def reference_order(q: OrcQuery) -> list[int]:
     return list(out[:q.k])
 
 
-def count(g: Graph, q: OrcQuery, order=None, filters=3, threads=1, root_range=None) -> dict:
+def count(g: Graph, q: OrcQuery, order=None, filters=3, threads=1, root_range=None,
+          root_step=1) -> dict:
+    """Exact count over the level-0 candidates at bucket positions
+    begin, begin + root_step, ... below end (root_range None: the whole bucket)."""
     order = reference_order(q) if order is None else list(order)
     o = _u32(order)
     r = OrcResult()
     rb, re_ = (0, 2 ** 64 - 1) if root_range is None else root_range
-    rc = _lib.orc_count(g.h, C.byref(q), _p(o), filters, threads, rb, re_, C.byref(r))
+    rc = _lib.orc_count(g.h, C.byref(q), _p(o), filters, threads, rb, re_, max(1, root_step),
+                        C.byref(r))
     if rc:
         raise RuntimeError(f"oracle count failed: {rc}")
     return {"count": r.count, "level_rows": list(r.level_rows[:q.k + 1]), "balg": r.balg,
@@ -154,3 +170,93 @@ def emit(g: Graph, q: OrcQuery, order=None, filters=3, cap=None) -> np.ndarray:
 
 def bucket_size(g: Graph, q: OrcQuery, order) -> int:
     return _lib.orc_bucket_size(g.h, C.byref(q), _p(_u32(order)))
+
+
+# ---- checker-side generators (oracle/gen.c) ---------------------------------------
+class PlainGraph:
+    """Symmetrised data graph as plain sorted CSR arrays (identity ids), built by
+    oracle/gen.c without the product library."""
+
+    def __init__(self, n, off, adj, labels):
+        self.n, self.off, self.adj, self.labels = n, off, adj, labels
+
+    @property
+    def m(self):
+        return int(self.off[-1])
+
+    def oracle_graph(self) -> Graph:
+        gid = np.arange(self.n, dtype=np.uint32)
+        return Graph.from_arrays(self.n, self.n - 1, gid, self.off, self.adj, self.off,
+                                 self.adj, self.labels)
+
+    def degree(self):
+        return np.diff(self.off.astype(np.int64))
+
+
+def _take(p, size):
+    out = np.ctypeslib.as_array(p, shape=(max(size, 1),))[:size].copy()
+    _libc.free(C.cast(p, C.c_void_p))
+    return out
+
+
+def gen_labels(n, L, kind="uniform", s=1.0, seed=1):
+    out = np.zeros(n, dtype=np.uint32)
+    rc = _lib.orc_gen_labels(n, 0 if kind == "uniform" else 1, L, s, seed, _p(out))
+    if rc:
+        raise RuntimeError(f"oracle labels failed: {rc}")
+    return out
+
+
+def rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=0, n_labels=32, label_kind="zipf",
+         zipf_s=1.0, label_seed=1, threads=None) -> PlainGraph:
+    """Symmetrised R-MAT graph (self-loops and repeats removed, ids not permuted)."""
+    threads = threads or os.cpu_count() or 1
+    op, ap, m = P32(), P32(), C.c_uint64()
+    rc = _lib.orc_gen_rmat_csr(scale, edge_factor, a, b, c, seed, threads, C.byref(op),
+                               C.byref(ap), C.byref(m))
+    if rc:
+        raise RuntimeError(f"oracle rmat failed: {rc}")
+    n = 1 << scale
+    off, adj = _take(op, n + 1), _take(ap, m.value)
+    return PlainGraph(n, off, adj, gen_labels(n, n_labels, label_kind, zipf_s, label_seed))
+
+
+def _masks(k, edges):
+    adjm = np.zeros(16, dtype=np.uint32)
+    for u, w in edges:
+        adjm[u] |= 1 << w
+        adjm[w] |= 1 << u
+    return adjm
+
+
+def walk_labels(g: PlainGraph, k, edges, seed, stream=0x57414C4B):
+    """Query labels copied from a random walk on g along the BFS tree of the query."""
+    out = np.zeros(16, dtype=np.uint32)
+    rc = _lib.orc_walk_labels(g.n, _p(g.off), _p(g.adj), _p(g.labels), k, _p(_masks(k, edges)),
+                              seed, stream, _p(out))
+    if rc:
+        raise RuntimeError(f"oracle walk failed: {rc}")
+    return out[:k].tolist()
+
+
+def random_query_edges(k, p_extra, seed):
+    """Edges of a random connected query (spanning tree + extra pairs)."""
+    adjm = np.zeros(16, dtype=np.uint32)
+    rc = _lib.orc_random_query_shape(k, p_extra, seed, _p(adjm))
+    if rc:
+        raise RuntimeError(f"oracle random query failed: {rc}")
+    return [(u, w) for u in range(k) for w in range(u + 1, k) if adjm[u] >> w & 1]
+
+
+def query_from_edges(k, edges, labels) -> OrcQuery:
+    """Symmetrised query over local ids 0..k-1 with sorted adjacency."""
+    nb = [set() for _ in range(k)]
+    for u, w in edges:
+        nb[u].add(w)
+        nb[w].add(u)
+    off = np.zeros(k + 1, dtype=np.uint32)
+    adj = []
+    for u in range(k):
+        adj += sorted(nb[u])
+        off[u + 1] = len(adj)
+    return make_query(k, np.arange(k), off, adj or [0], labels)

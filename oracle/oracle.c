@@ -36,6 +36,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 #define ORC_MAXK 16
 #define ORC_OK 0
@@ -105,6 +106,71 @@ void orc_graph_free(orc_graph* g) {
   free(g);
 }
 
+/* Vertex-parallel loop: fn(ctx, v) for v in [0, n) over the host's cores,
+ * in interleaved blocks of 256 vertices. */
+typedef struct par_job {
+  uint32_t n, t, nt;
+  void (*fn)(void*, uint32_t);
+  void* ctx;
+} par_job;
+
+static void* par_run(void* arg) {
+  par_job* J = (par_job*)arg;
+  for (uint64_t b = (uint64_t)J->t * 256; b < J->n; b += (uint64_t)J->nt * 256) {
+    uint64_t e = b + 256 < J->n ? b + 256 : J->n;
+    for (uint64_t v = b; v < e; ++v) J->fn(J->ctx, (uint32_t)v);
+  }
+  return NULL;
+}
+
+static void par_for(uint32_t n, void (*fn)(void*, uint32_t), void* ctx) {
+  long h = sysconf(_SC_NPROCESSORS_ONLN);
+  uint32_t nt = h < 1 ? 1 : (uint32_t)(h > 256 ? 256 : h);
+  if (n < 4096) nt = 1;
+  par_job jobs[256];
+  pthread_t th[256];
+  for (uint32_t t = 0; t < nt; ++t) {
+    jobs[t].n = n;
+    jobs[t].t = t;
+    jobs[t].nt = nt;
+    jobs[t].fn = fn;
+    jobs[t].ctx = ctx;
+  }
+  if (nt == 1) {
+    par_run(&jobs[0]);
+    return;
+  }
+  for (uint32_t t = 0; t < nt; ++t) pthread_create(&th[t], NULL, par_run, &jobs[t]);
+  for (uint32_t t = 0; t < nt; ++t) pthread_join(th[t], NULL);
+}
+
+typedef struct norm_ctx {
+  const uint32_t *off, *edges, *g2l;
+  uint32_t max_vid;
+  uint32_t* a;
+  uint64_t* uniq;
+  atomic_int bad;
+} norm_ctx;
+
+static void norm_vertex(void* p, uint32_t v) {
+  norm_ctx* c = (norm_ctx*)p;
+  const uint64_t s = c->off[v], e = c->off[v + 1];
+  for (uint64_t j = s; j < e; ++j) {
+    const uint32_t gid = c->edges[j];
+    if (gid > c->max_vid || c->g2l[gid] == UINT32_MAX) {
+      atomic_store(&c->bad, 1);
+      c->uniq[v] = 0;
+      return;
+    }
+    c->a[j] = c->g2l[gid];
+  }
+  qsort(c->a + s, e - s, 4, cmp_u32);
+  uint64_t u = s;
+  for (uint64_t j = s; j < e; ++j)
+    if (j == s || c->a[j] != c->a[j - 1]) c->a[u++] = c->a[j];
+  c->uniq[v] = u - s;
+}
+
 /* Local adjacency of one direction: map ids, sort, drop repeats. */
 static int normalise_dir(uint32_t n, const uint32_t* off, const uint32_t* edges,
                          const uint32_t* g2l, uint32_t max_vid, uint64_t** noff,
@@ -113,29 +179,51 @@ static int normalise_dir(uint32_t n, const uint32_t* off, const uint32_t* edges,
   uint64_t* o = (uint64_t*)calloc((size_t)n + 1, 8);
   uint32_t* a = (uint32_t*)malloc((m ? m : 1) * 4);
   if (!o || !a) return ORC_E_OOM;
+  norm_ctx c = {off, edges, g2l, max_vid, a, o, 0};
+  par_for(n, norm_vertex, &c); /* o[v] = distinct entries of v */
+  if (atomic_load(&c.bad)) {
+    free(o);
+    free(a);
+    return ORC_E_FORMAT;
+  }
   uint64_t w = 0;
   for (uint32_t v = 0; v < n; ++v) {
+    const uint64_t u = o[v];
+    if (w != off[v]) memmove(a + w, a + off[v], u * 4);
     o[v] = w;
-    uint64_t s = w;
-    for (uint64_t e = off[v]; e < off[v + 1]; ++e) {
-      uint32_t gid = edges[e];
-      if (gid > max_vid || g2l[gid] == UINT32_MAX) {
-        free(o);
-        free(a);
-        return ORC_E_FORMAT;
-      }
-      a[w++] = g2l[gid];
-    }
-    qsort(a + s, w - s, 4, cmp_u32);
-    uint64_t u = s;
-    for (uint64_t e = s; e < w; ++e)
-      if (e == s || a[e] != a[e - 1]) a[u++] = a[e];
-    w = u;
+    w += u;
   }
   o[n] = w;
   *noff = o;
   *nadj = a;
   return ORC_OK;
+}
+
+typedef struct slice_ctx {
+  orc_graph* g;
+  int d;
+  const uint64_t* off;
+  uint32_t* adj;
+} slice_ctx;
+
+/* One vertex's list ordered by (label, id), its label-slice starts, degree,
+ * neighbour-label bits and self-loop flag. */
+static void slice_vertex(void* p, uint32_t v) {
+  slice_ctx* c = (slice_ctx*)p;
+  orc_graph* g = c->g;
+  const int d = c->d;
+  const uint32_t L = g->L, W = g->W;
+  const uint64_t s = c->off[v], e = c->off[v + 1];
+  g->deg[d][v] = (uint32_t)(e - s);
+  for (uint64_t j = s; j < e; ++j)
+    if (c->adj[j] == v) g->self[v] = 1;
+  qsort(c->adj + s, e - s, 4, cmp_lab_id);
+  uint64_t q = s;
+  for (uint32_t l = 0; l < L; ++l) {
+    g->loff[d][(uint64_t)v * L + l] = q;
+    while (q < e && g->label[c->adj[q]] == l) ++q;
+    if (g->loff[d][(uint64_t)v * L + l] < q) g->nlb[d][(uint64_t)v * W + l / 32] |= 1u << (l % 32);
+  }
 }
 
 orc_graph* orc_graph_from_arrays(uint32_t n, uint32_t max_vid, const uint32_t* globalid,
@@ -187,13 +275,21 @@ orc_graph* orc_graph_from_arrays(uint32_t n, uint32_t max_vid, const uint32_t* g
   uint64_t* off[2];
   uint32_t* adj[2];
   int rc = normalise_dir(n, out_off, out_edges, g2l, max_vid, &off[0], &adj[0]);
-  if (rc == ORC_OK) rc = normalise_dir(n, in_off, in_edges, g2l, max_vid, &off[1], &adj[1]);
+  const int same_arrays = in_off == out_off && in_edges == out_edges;
+  if (rc == ORC_OK && !same_arrays)
+    rc = normalise_dir(n, in_off, in_edges, g2l, max_vid, &off[1], &adj[1]);
   if (rc) {
     *err = rc;
     goto fail;
   }
-  g->symmetric = off[0][n] == off[1][n] && memcmp(off[0], off[1], ((size_t)n + 1) * 8) == 0 &&
-                 memcmp(adj[0], adj[1], off[0][n] * 4) == 0;
+  if (same_arrays) {
+    g->symmetric = 1;
+    off[1] = NULL;
+    adj[1] = NULL;
+  } else {
+    g->symmetric = off[0][n] == off[1][n] && memcmp(off[0], off[1], ((size_t)n + 1) * 8) == 0 &&
+                   memcmp(adj[0], adj[1], off[0][n] * 4) == 0;
+  }
   g->self = (uint8_t*)calloc(n, 1);
   for (int d = 0; d < 2; ++d) {
     if (d == 1 && g->symmetric) {
@@ -210,19 +306,8 @@ orc_graph* orc_graph_from_arrays(uint32_t n, uint32_t max_vid, const uint32_t* g
     g->deg[d] = (uint32_t*)malloc((size_t)n * 4);
     g->nlb[d] = (uint32_t*)calloc((size_t)n * W, 4);
     g_sort_labels = g->label;
-    for (uint32_t v = 0; v < n; ++v) {
-      uint64_t s = off[d][v], e = off[d][v + 1];
-      g->deg[d][v] = (uint32_t)(e - s);
-      for (uint64_t j = s; j < e; ++j)
-        if (adj[d][j] == v) g->self[v] = 1;
-      qsort(adj[d] + s, e - s, 4, cmp_lab_id);
-      uint64_t p = s;
-      for (uint32_t l = 0; l < L; ++l) {
-        g->loff[d][(uint64_t)v * L + l] = p;
-        while (p < e && g->label[adj[d][p]] == l) ++p;
-        if (g->loff[d][(uint64_t)v * L + l] < p) g->nlb[d][(uint64_t)v * W + l / 32] |= 1u << (l % 32);
-      }
-    }
+    slice_ctx sc = {g, d, off[d], adj[d]};
+    par_for(n, slice_vertex, &sc);
     g->loff[d][(uint64_t)n * L] = off[d][n];
     g->adj[d] = adj[d];
     free(off[d]);
@@ -477,8 +562,8 @@ typedef struct shared_ctx {
   uint32_t* emit_rows;
   uint64_t emit_cap;
   uint64_t emit_n;
-  atomic_ullong next_root;
-  uint64_t root_begin, root_end;
+  atomic_ullong next_root; /* index j of the next root position begin + j*step */
+  uint64_t root_begin, root_end, root_step;
 } shared_ctx;
 
 typedef struct thread_ctx {
@@ -595,8 +680,9 @@ static void* worker(void* arg) {
   const uint32_t lab = P->label[0];
   const uint32_t b0 = g->bucket_off[lab];
   for (;;) {
-    uint64_t r = atomic_fetch_add(&S->next_root, 1);
-    if (r >= S->root_end) break;
+    const uint64_t j = atomic_fetch_add(&S->next_root, 1);
+    if (j >= (S->root_end - S->root_begin + S->root_step - 1) / S->root_step) break;
+    const uint64_t r = S->root_begin + j * S->root_step;
     uint32_t x = g->bucket_vid[b0 + r];
     if (!passes(T, 0, x)) continue;
     T->rows[1]++;
@@ -608,8 +694,8 @@ static void* worker(void* arg) {
 }
 
 static int run(const orc_graph* g, const orc_query* q, const uint32_t* order, uint32_t filters,
-               int threads, uint64_t root_begin, uint64_t root_end, uint32_t* emit_rows,
-               uint64_t emit_cap, orc_result* res, uint64_t* emitted) {
+               int threads, uint64_t root_begin, uint64_t root_end, uint64_t root_step,
+               uint32_t* emit_rows, uint64_t emit_cap, orc_result* res, uint64_t* emitted) {
   plan P;
   int rc = make_plan(g, q, order, &P);
   if (rc) return rc;
@@ -628,7 +714,8 @@ static int run(const orc_graph* g, const orc_query* q, const uint32_t* order, ui
   S.emit_cap = emit_cap;
   S.root_begin = root_begin;
   S.root_end = root_end;
-  atomic_init(&S.next_root, root_begin);
+  S.root_step = root_step < 1 ? 1 : root_step;
+  atomic_init(&S.next_root, 0);
   if (threads < 1) threads = 1;
   if (emit_rows) threads = 1;
   thread_ctx* T = (thread_ctx*)calloc((size_t)threads, sizeof(thread_ctx));
@@ -640,8 +727,9 @@ static int run(const orc_graph* g, const orc_query* q, const uint32_t* order, ui
   if (threads == 1) worker(&T[0]);
   else
     for (int t = 0; t < threads; ++t) pthread_join(th[t], NULL);
-  /* level-0 charge over the whole label bucket (root sampling scales it) */
-  res->balg = res->balg_count = (root_end - root_begin) * (12ull + 4ull * g->W);
+  /* level-0 charge: one candidate test per root position taken */
+  res->balg = res->balg_count =
+      ((root_end - root_begin + S.root_step - 1) / S.root_step) * (12ull + 4ull * g->W);
   for (int t = 0; t < threads; ++t) {
     res->count += T[t].count;
     res->balg += T[t].balg;
@@ -654,9 +742,12 @@ static int run(const orc_graph* g, const orc_query* q, const uint32_t* order, ui
   return ORC_OK;
 }
 
+/* Count over the level-0 candidates at bucket positions root_begin,
+ * root_begin + root_step, ... below root_end (root_step 0 or 1: all). */
 int orc_count(const orc_graph* g, const orc_query* q, const uint32_t* order, uint32_t filters,
-              int threads, uint64_t root_begin, uint64_t root_end, orc_result* res) {
-  return run(g, q, order, filters, threads, root_begin, root_end, NULL, 0, res, NULL);
+              int threads, uint64_t root_begin, uint64_t root_end, uint64_t root_step,
+              orc_result* res) {
+  return run(g, q, order, filters, threads, root_begin, root_end, root_step, NULL, 0, res, NULL);
 }
 
 static uint32_t g_row_k;
@@ -672,7 +763,7 @@ static int cmp_rows(const void* a, const void* b) {
 int orc_emit(const orc_graph* g, const orc_query* q, const uint32_t* order, uint32_t filters,
              uint32_t* rows, uint64_t cap, uint64_t* n_rows) {
   orc_result res;
-  int rc = run(g, q, order, filters, 1, 0, UINT64_MAX, rows, cap, &res, n_rows);
+  int rc = run(g, q, order, filters, 1, 0, UINT64_MAX, 1, rows, cap, &res, n_rows);
   if (rc) return rc;
   g_row_k = q->k;
   qsort(rows, *n_rows < cap ? *n_rows : cap, (size_t)q->k * 4, cmp_rows);

@@ -1,6 +1,7 @@
-"""The N>1 host path of bench.py on CPU: two gloo ranks shard every query's
-level-0 candidates with shard_roots, count their shard (the oracle stands in
-for each rank's GPU) and sum with one all-reduce; the sum is the full count."""
+"""The N>1 host path of bench.py on CPU: two gloo ranks take every second
+level-0 candidate of each query (shard_strided), count their shard (the
+oracle stands in for each rank's GPU) and sum with one all-reduce; the sum is
+the full count, for single queries and for a batch's per-query vector."""
 import os
 import socket
 
@@ -24,16 +25,18 @@ def _port():
 def _rank(rank, world, port, out):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
-    g = mg.chung_lu(2000, avg_deg=8, n_labels=4)
+    g = mg.rmat(11, 8, n_labels=8)
     qs = [mg.query_walk(g, s, seed=2 + i) for i, s in enumerate(mg.SHAPES)]
-    sizes = mg.level0_sizes(g, qs)
+    qs += [mg.query_random(g, 3 + i % 3, 0.3, seed=1000 + i) for i in range(8)]
     og = O.Graph.from_csr(g)
+    sh = mg.shard_strided(rank, world)
     local = []
-    for q, n in zip(qs, sizes):
-        lo, hi = mg.shard_roots(n, rank, world)
-        local.append(O.count(og, O.query_from_csr(q), root_range=(lo, hi))["count"])
+    for q in qs:
+        b = sh["root_range"][0]
+        local.append(O.count(og, O.query_from_csr(q), root_range=(b, 2 ** 63),
+                             root_step=sh["root_step"])["count"])
     t = torch.tensor(local, dtype=torch.int64)
-    dist.all_reduce(t)
+    dist.all_reduce(t)  # the one exchange: the per-query count vector
     if rank == 0:
         full = [O.count(og, O.query_from_csr(q))["count"] for q in qs]
         np.save(out, np.array([t.tolist(), full], dtype=np.int64))
@@ -41,9 +44,28 @@ def _rank(rank, world, port, out):
     dist.destroy_process_group()
 
 
-def test_two_rank_sharded_counts_sum_to_full(tmp_path):
+def test_two_rank_strided_counts_sum_to_full(tmp_path):
     out = str(tmp_path / "r.npy")
     mp.spawn(_rank, args=(2, _port(), out), nprocs=2, join=True)
     summed, full = np.load(out)
     assert summed.tolist() == full.tolist()
     assert sum(full) > 0
+
+
+def test_strided_shards_partition_and_balance_a_hub_first_bucket():
+    """On an R-MAT bucket (hubs first) contiguous halves give rank 0 most of
+    the adjacency volume of the roots; the stride splits it nearly evenly."""
+    g = mg.rmat(14, n_labels=4)
+    lab = g.array("labels")
+    deg = np.diff(g.array("out_off").astype(np.int64))
+    bucket = np.flatnonzero(lab == 0)  # ascending ids, as the engine's bucket
+    for world in (2, 4, 8):
+        parts = [np.arange(len(bucket))[mg.shard_strided(r, world)["root_range"][0]::world]
+                 for r in range(world)]
+        assert sorted(np.concatenate(parts).tolist()) == list(range(len(bucket)))
+        strided = [deg[bucket[p]].sum() for p in parts]
+        contiguous = [deg[bucket[lo:hi]].sum() for lo, hi in
+                      (mg.shard_roots(len(bucket), r, world) for r in range(world))]
+        assert max(strided) / np.mean(strided) < 1.25, (world, strided)
+        assert max(contiguous) / np.mean(contiguous) > 1.5, (world, contiguous)
+    assert mg.shard_strided(0, 1) == {}

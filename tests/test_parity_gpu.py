@@ -286,3 +286,62 @@ def test_batch_orders_level_rows_and_budget(c1):
     for cb, cs_ in zip(counts_b, singles):
         assert cb == cs_ or cb == 2 ** 64 - 1
     assert any(cb == 2 ** 64 - 1 for cb in counts_b)
+
+
+@pytest.fixture(scope="module")
+def rmat20():
+    """R-MAT scale 20 (1,048,576 vertices, edge factor 16, 32 Zipf labels): the
+    C2 generator one scale down, with the five C2 query shapes."""
+    g = mg.rmat(20)
+    qs = [mg.query_walk(g, s, seed=2 + i) for i, s in enumerate(mg.SHAPES)]
+    og = O.Graph.from_csr(g)
+    dg = mg.DeviceGraph(g)
+    yield g, qs, og, dg
+    dg.free()
+
+
+def test_rmat20_sampled_roots_all_shapes_both_tail_modes(rmat20):
+    """Counts, per-prefix survivors P_i and algorithmic bytes of strided root
+    samples (hubs included for all but the 4-cycle, whose top hub alone takes
+    the oracle tens of seconds) equal the oracle's, with the closed-form
+    pendant tail on and off."""
+    g, qs, og, dg = rmat20
+    threads = os.cpu_count() or 1
+    for name, q in zip(mg.SHAPES, qs):
+        oq = O.query_from_csr(q)
+        order = O.reference_order(oq)
+        nb = O.bucket_size(og, oq, order)
+        first = 5 if name == "4-cycle" else 0
+        for b, s in ((first, max(1, nb // 4096)), (3, max(1, nb // 8192))):
+            want = O.count(og, oq, order=order, threads=threads, root_range=(b, nb),
+                           root_step=s)
+            assert want["count"] > 0, name
+            for no_tail in (0, 1):
+                c, st = dg.count(q, stats=True, root_range=(b, nb), root_step=s,
+                                 no_tail=no_tail)
+                assert c == want["count"], (name, b, s, no_tail)
+                assert st["level_rows"] == want["level_rows"], (name, b, s, no_tail)
+                assert st["balg_bytes"] == want["balg"], (name, b, s, no_tail)
+                assert st["balg_count_bytes"] == want["balg_count"], (name, b, s, no_tail)
+
+
+def test_root_step_partitions_and_matches_oracle():
+    g = mg.chung_lu(3000, avg_deg=8, n_labels=3)
+    og = O.Graph.from_csr(g)
+    dg = mg.DeviceGraph(g)
+    try:
+        for i, shape in enumerate(mg.SHAPES):
+            q = mg.query_walk(g, shape, seed=40 + i)
+            oq = O.query_from_csr(q)
+            full = dg.count(q)
+            assert full == O.count(og, oq)["count"]
+            for world in (2, 3, 7):
+                parts = [dg.count(q, **mg.shard_strided(r, world)) for r in range(world)]
+                assert sum(parts) == full, (shape, world)
+            for b, e, s in ((0, 10 ** 9, 5), (7, 400, 3), (11, 12, 4), (0, 0, 9)):
+                want = O.count(og, oq, root_range=(b, e if e else 2 ** 63), root_step=s)
+                assert dg.count(q, root_range=(b, e), root_step=s) == want["count"]
+            rows = dg.emit(q, root_range=(2, 10 ** 9), root_step=4)
+            assert len(rows) == O.count(og, oq, root_range=(2, 2 ** 63), root_step=4)["count"]
+    finally:
+        dg.free()
