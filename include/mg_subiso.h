@@ -140,7 +140,23 @@ typedef struct mg_graph_info {
   uint64_t device_bytes;     /* resident bytes of graph + derived indices    */
   uint32_t max_degree;
   uint32_t nlb_words;        /* W = ceil(n_labels / 32)                       */
+  uint32_t hubs;             /* vertices with a dense neighbour bitmap        */
+  uint32_t hub_min_degree;   /* smallest degree among them                    */
+  uint64_t hub_bytes;        /* device bytes of the hub bitmaps               */
 } mg_graph_info;
+
+/* Options of mg_graph_upload_ex.  Hub bitmaps: the highest-degree vertices
+ * get one bit per data vertex over their whole adjacency, so testing whether
+ * a candidate lies in a hub's label slice is one load instead of a binary
+ * search.  Vertices are taken in decreasing degree while the budget lasts
+ * (ties at the cut are all taken or all left out).                        */
+#define MG_HUB_AUTO (~(uint64_t)0)
+typedef struct mg_upload_opts {
+  uint64_t hub_bytes;        /* MG_HUB_AUTO: min(1 GiB, free device memory/8);
+                                0: no hub bitmaps                            */
+  uint32_t hub_min_degree;   /* smallest degree of a hub; 0 = 128             */
+  uint32_t _reserved;        /* must be 0                                    */
+} mg_upload_opts;
 
 /* ---- library ------------------------------------------------------------ */
 const char* mg_last_error(void);
@@ -223,6 +239,9 @@ int  mg_plan_order(void* dgraph, const mg_csr_view* q, const mg_opts* opts,
  * the UnifiedOwnedBuffer::Init uploads of WOJSubIsoKernelWrapper::Filter
  * (core/task/gpu_task/kernel/kernel_woj_subsio.cu:753-815).               */
 int  mg_graph_upload(const mg_csr_view* g, int device, void** dgraph);
+/* The same with explicit options (NULL = defaults, as mg_graph_upload).     */
+int  mg_graph_upload_ex(const mg_csr_view* g, int device, const mg_upload_opts* opts,
+                        void** dgraph);
 void mg_graph_free(void* dgraph);
 int  mg_graph_get_info(void* dgraph, mg_graph_info* info);
 

@@ -77,7 +77,16 @@ class GraphInfo(C.Structure):
     _fields_ = [("n", C.c_uint32), ("n_labels", C.c_uint32), ("m_out", C.c_uint64),
                 ("m_in", C.c_uint64), ("symmetric", C.c_uint32), ("device", C.c_uint32),
                 ("device_bytes", C.c_uint64), ("max_degree", C.c_uint32),
-                ("nlb_words", C.c_uint32)]
+                ("nlb_words", C.c_uint32), ("hubs", C.c_uint32),
+                ("hub_min_degree", C.c_uint32), ("hub_bytes", C.c_uint64)]
+
+
+MG_HUB_AUTO = 2 ** 64 - 1
+
+
+class UploadOpts(C.Structure):
+    _fields_ = [("hub_bytes", C.c_uint64), ("hub_min_degree", C.c_uint32),
+                ("_reserved", C.c_uint32)]
 
 
 class MGError(RuntimeError):
@@ -121,6 +130,7 @@ _SIGS = {
     "mg_graph_upload": (C.c_int, [_PV, C.c_int, _PVP]),
     "mg_graph_free": (None, [_VP]),
     "mg_graph_get_info": (C.c_int, [_VP, C.POINTER(GraphInfo)]),
+    "mg_graph_upload_ex": (C.c_int, [_PV, C.c_int, C.POINTER(UploadOpts), _PVP]),
     "mg_subiso_count": (C.c_int, [_VP, _PV, C.POINTER(Opts), _PU64]),
     "mg_subiso_count_ex": (C.c_int, [_VP, _PV, C.POINTER(Opts), _PU64, C.POINTER(Stats)]),
     "mg_subiso_emit": (C.c_int, [_VP, _PV, C.POINTER(Opts), P32, C.c_uint64, _PU64]),

@@ -26,7 +26,8 @@ constexpr uint32_t ERR_TIMEOUT = 4u;    // a bounded device wait gave up
 //   nlb[d]   : n*W neighbour-label bits (bit l: v has a d-neighbour labelled l)
 //   deg[d]   : distinct d-neighbours
 //   label    : compact labels 0..L-1
-//   bucket_* : vertices grouped by label (ascending id inside a bucket)
+//   bucket_* : vertices grouped by label (ascending id inside a bucket);
+//              bucket_pos[v] = index of v inside its bucket
 //   selfbits : bit v set when (v, v) is an edge
 //   globalid : local id -> global id of the reference format
 struct GraphDev {
@@ -38,9 +39,17 @@ struct GraphDev {
   const uint32_t* label;
   const uint32_t* bucket_off;
   const uint32_t* bucket_vid;
+  const uint32_t* bucket_pos;  // position of every vertex inside its label bucket
   const uint32_t* selfbits;
   const uint32_t* globalid;
+  // Hub bitmaps per direction (nullptr: none): hub_slot[d][v] is v's row in
+  // hub_bits[d] or NO_HUB; a row holds hub_words words, bit x set when x is a
+  // d-neighbour of v.
+  const uint16_t* hub_slot[2];
+  const uint32_t* hub_bits[2];
+  uint32_t hub_words;
 };
+constexpr uint16_t NO_HUB = 0xFFFF;
 
 // Matching plan of one query for one order.  Position i matches query vertex
 // perm[i].  cons[i][c] = pos | dir << 8: the candidate for position i must be
@@ -76,6 +85,9 @@ struct PlanDev {
 // memoised aggregates.
 struct TailKey {
   uint32_t da, la, db, lb;
+  uint32_t lp;     // label of m_p (dense aggregates cover this label's bucket)
+  uint32_t pad;
+  uint64_t base;   // first entry of this key in the dense aggregate arrays
 };
 
 struct Workspace;  // enumeration scratch (mg_enum.cu)

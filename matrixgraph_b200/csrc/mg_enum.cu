@@ -61,6 +61,9 @@ struct Workspace {
   uint64_t hsize = 0;
   TailKey* tkeys = nullptr;
   uint32_t tkeys_cap = 0;
+  unsigned long long* tdA = nullptr;   // dense aggregates (tail keys' buckets)
+  unsigned long long* tdAD = nullptr;
+  uint64_t td_cap = 0;
   unsigned long long* ctr = nullptr;     // device counters
   unsigned long long* h_ctr = nullptr;   // pinned mirror
   unsigned long long* counts = nullptr;  // per query
@@ -198,6 +201,11 @@ struct StepArgs {
   uint32_t* hnew;
   uint64_t hmask;
   const TailKey* tkeys;
+  // Dense two-hop aggregates (tail_dense): entry tkeys[kid].base +
+  // bucket_pos[m_p]; the tail is then counted while expanding position k-3.
+  uint32_t tail_dense;
+  const unsigned long long* tdA;
+  const unsigned long long* tdAD;
 };
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -223,6 +231,33 @@ __device__ __forceinline__ void slice_of(const GraphDev& g, uint32_t dir, uint32
   const uint32_t* p = g.loff[dir] + uint64_t(y) * g.L + lab;
   s = __ldg(p);
   e = __ldg(p + 1);
+}
+
+// x in the d-adjacency of y, where x is known to carry the label of the slice
+// [s, e) of y being asked about: a hub's bitmap answers with one load, any
+// other vertex by binary search in the slice.
+__device__ __forceinline__ bool in_slice_se(const GraphDev& g, uint32_t d, uint32_t y, uint32_t s,
+                                            uint32_t e, uint32_t x) {
+  if (g.hub_slot[d]) {
+    const uint16_t h = __ldg(g.hub_slot[d] + y);
+    if (h != NO_HUB)
+      return (__ldg(g.hub_bits[d] + uint64_t(h) * g.hub_words + (x >> 5)) >> (x & 31)) & 1u;
+  }
+  return contains(g.adj[d], s, e, x);
+}
+
+// x (labelled lab) in the label-lab slice of y's d-adjacency; a hub needs no
+// slice offsets at all.
+__device__ __forceinline__ bool in_slice(const GraphDev& g, uint32_t d, uint32_t y, uint32_t lab,
+                                         uint32_t x) {
+  if (g.hub_slot[d]) {
+    const uint16_t h = __ldg(g.hub_slot[d] + y);
+    if (h != NO_HUB)
+      return (__ldg(g.hub_bits[d] + uint64_t(h) * g.hub_words + (x >> 5)) >> (x & 31)) & 1u;
+  }
+  uint32_t s, e;
+  slice_of(g, d, y, lab, s, e);
+  return contains(g.adj[d], s, e, x);
 }
 
 __device__ __forceinline__ bool pass_filters(const GraphDev& g, const PlanDev& P, uint32_t i,
@@ -289,13 +324,15 @@ __device__ __forceinline__ bool tail_row(const StepArgs& a, const PlanDev& P) {
 }
 
 // Adds a thread's accumulated match count and prefix survivors of query q:
-// s1 prefixes of length i+1 and sk prefixes of length k (closed-form counts).
+// s1 prefixes of length i+1, s2 of length i+2 and sk of length k (the last
+// two from closed-form counts).
 __device__ __forceinline__ void acc_flush(const StepArgs& a, uint32_t q, uint32_t i,
                                           unsigned long long cnt, unsigned long long s1,
-                                          unsigned long long sk) {
+                                          unsigned long long sk, unsigned long long s2 = 0) {
   if (cnt) atomicAdd(&a.counts[q], cnt);
   unsigned long long* L = a.lvl_rows + uint64_t(q) * (MAXK + 1);
   if (s1) atomicAdd(&L[i + 1], s1);
+  if (s2) atomicAdd(&L[i + 2], s2);
   if (sk) atomicAdd(&L[a.plans[q].k], sk);
 }
 
@@ -304,15 +341,17 @@ __device__ __forceinline__ void acc_flush(const StepArgs& a, uint32_t q, uint32_
 __device__ __forceinline__ void acc_flush_warp(const StepArgs& a, uint32_t q, uint32_t i,
                                                unsigned long long& cnt,
                                                unsigned long long& s1,
-                                               unsigned long long& sk, bool force) {
+                                               unsigned long long& sk,
+                                               unsigned long long& s2, bool force) {
   const bool uniform = __all_sync(FULL, q == __shfl_sync(FULL, q, 0));
   if (uniform) {
-    const unsigned long long c = warp_sum(cnt), x = warp_sum(s1), y = warp_sum(sk);
-    if ((threadIdx.x & 31) == 0) acc_flush(a, q, i, c, x, y);
-    cnt = s1 = sk = 0;
+    const unsigned long long c = warp_sum(cnt), x = warp_sum(s1), y = warp_sum(sk),
+                             z = warp_sum(s2);
+    if ((threadIdx.x & 31) == 0) acc_flush(a, q, i, c, x, y, z);
+    cnt = s1 = sk = s2 = 0;
   } else if (force) {
-    acc_flush(a, q, i, cnt, s1, sk);
-    cnt = s1 = sk = 0;
+    acc_flush(a, q, i, cnt, s1, sk, s2);
+    cnt = s1 = sk = s2 = 0;
   }
 }
 
@@ -341,6 +380,36 @@ __global__ void __launch_bounds__(256) k_tail_collect(StepArgs a) {
       }
       if (old == key) break;
       slot = (slot + 1) & a.hmask;
+    }
+  }
+}
+
+// Dense aggregates of one tail key over the whole label bucket of m_p, warp
+// per bucket position: tdA[base + j], tdAD[base + j] for y = bucket_vid[j].
+__global__ void __launch_bounds__(256) k_tail_dense(GraphDev g, TailKey tk, uint32_t nb,
+                                                    unsigned long long* tdA,
+                                                    unsigned long long* tdAD) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5;
+  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  const uint32_t b0 = __ldg(g.bucket_off + tk.lp);
+  for (uint64_t j = warp; j < nb; j += nwarps) {
+    const uint32_t y = __ldg(g.bucket_vid + b0 + j);
+    uint32_t s, e;
+    slice_of(g, tk.da, y, tk.la, s, e);
+    unsigned long long sa = 0, sd = 0;
+    for (uint32_t q = s + lane; q < e; q += 32) {
+      const uint32_t x = __ldg(g.adj[tk.da] + q);
+      uint32_t xs, xe;
+      slice_of(g, tk.db, x, tk.lb, xs, xe);
+      sd += xe - xs;
+      sa += xe - xs - ((tk.la == tk.lb && has_self(g, x)) ? 1u : 0u);
+    }
+    sa = warp_sum(sa);
+    sd = warp_sum(sd);
+    if (lane == 0) {
+      tdA[tk.base + j] = sa;
+      tdAD[tk.base + j] = sd;
     }
   }
 }
@@ -381,32 +450,30 @@ __global__ void __launch_bounds__(256) k_tail_compute(StepArgs a, uint64_t first
 // Work kernel: per row, the driving slice (shortest backward slice, or the
 // label bucket for a position without backward neighbours) and the
 // algorithmic-byte charge of extending the row.
-// Closed-form count of one row of prefix length a = k-2 under a two-position
+// Closed-form count of one prefix of length a = k-2 under a two-position
 // pendant tail (PlanDev::tail2).  With I the matched prefix, S = the
-// label-l_a slice of m_p, D(x) = |N_{l_b}(x)| and c(x) = D(x) - [x has a
-// self-loop and l_a == l_b], and A(y) = sum_{x in S(y)} c(x):
+// label-l_a slice [s, e) of m_p, D(x) = |N_{l_b}(x)| and c(x) = D(x) - [x has
+// a self-loop and l_a == l_b], and A(y) = sum_{x in S(y)} c(x),
+// AD(y) = sum_{x in S(y)} D(x):
 //   count = A(m_p) - sum_{i in Ia, m_i in S} (c(m_i) - #{j in J : m_j in N_{l_b}(m_i)})
 //           - sum_{j in J} |S|                   (every j in J is p itself)
 // Also returns the number of length-(k-1) prefixes |S \ I| and their
-// algorithmic bytes sum_{x in S \ I} D(x).
-__device__ __forceinline__ void tail_count(const StepArgs& a, const PlanDev& P, uint64_t r,
-                                           unsigned long long& cnt, unsigned long long& pre,
-                                           unsigned long long& dsum) {
+// algorithmic bytes sum_{x in S \ I} D(x).  col(j) is the vertex matched at
+// position j < a.
+template <class Col>
+__device__ __forceinline__ void tail_close(const StepArgs& a, const PlanDev& P, Col col,
+                                           uint32_t mp, uint32_t s, uint32_t e, long long c,
+                                           long long d, unsigned long long& cnt,
+                                           unsigned long long& pre, unsigned long long& dsum) {
   const GraphDev& g = a.g;
   const uint32_t ia = P.k - 2;
   const uint32_t la = P.label[ia], lb = P.label[ia + 1];
   const uint32_t da = P.tail_da, db = P.tail_db;
-  const uint32_t mp = a.in.col[P.tail_p][r];
-  uint32_t s, e;
-  slice_of(g, da, mp, la, s, e);
-  const uint64_t slot = memo_find(a, (uint64_t(P.tail_kid) << 32) | mp);
-  long long c = (long long)a.hA[slot];
-  long long d = (long long)a.hAD[slot];
   unsigned long long inS = 0;
   for (uint32_t mi = P.tail_Ia; mi; mi &= mi - 1) {
     const uint32_t i2 = __ffs(mi) - 1;
-    const uint32_t x = a.in.col[i2][r];
-    if (!contains(g.adj[da], s, e, x)) continue;
+    const uint32_t x = col(i2);
+    if (!in_slice_se(g, da, mp, s, e, x)) continue;
     inS += 1;
     uint32_t xs, xe;
     slice_of(g, db, x, lb, xs, xe);
@@ -415,7 +482,7 @@ __device__ __forceinline__ void tail_count(const StepArgs& a, const PlanDev& P, 
     if (la == lb && has_self(g, x)) cx -= 1;
     for (uint32_t mj = P.tail_J; mj; mj &= mj - 1) {
       const uint32_t j = __ffs(mj) - 1;
-      if (contains(g.adj[db], xs, xe, a.in.col[j][r])) cx -= 1;
+      if (in_slice_se(g, db, x, xs, xe, col(j))) cx -= 1;
     }
     c -= cx;
   }
@@ -425,6 +492,21 @@ __device__ __forceinline__ void tail_count(const StepArgs& a, const PlanDev& P, 
   dsum = (unsigned long long)d;
 }
 
+// Tail count of table row r from the memoised aggregates.
+__device__ __forceinline__ void tail_count(const StepArgs& a, const PlanDev& P, uint64_t r,
+                                           unsigned long long& cnt, unsigned long long& pre,
+                                           unsigned long long& dsum) {
+  const uint32_t mp = a.in.col[P.tail_p][r];
+  uint32_t s, e;
+  slice_of(a.g, P.tail_da, mp, P.label[P.k - 2], s, e);
+  const uint64_t slot = memo_find(a, (uint64_t(P.tail_kid) << 32) | mp);
+  tail_close(a, P, [&](uint32_t j) { return a.in.col[j][r]; }, mp, s, e,
+             (long long)a.hA[slot], (long long)a.hAD[slot], cnt, pre, dsum);
+}
+
+// Work kernel: per row, the driving slice (shortest backward slice, or the
+// label bucket for a position without backward neighbours) and the
+// algorithmic-byte charge of extending the row.
 __global__ void __launch_bounds__(256) k_work(StepArgs a) {
   unsigned long long bal = 0, balc = 0, tcnt = 0, tpre = 0;
   uint32_t tq = 0;
@@ -636,7 +718,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t span = a.t1 - a.t0;
   const uint64_t ntiles = (span + EXPAND_BLOCK - 1) / EXPAND_BLOCK;
-  unsigned long long cnt = 0, bal = 0, balc = 0, s1 = 0, sk = 0;
+  unsigned long long cnt = 0, bal = 0, balc = 0, s1 = 0, sk = 0, s2 = 0;
   uint32_t cnt_q = 0;
   // Device work queue: each block takes `grab` consecutive tiles at a time,
   // so a block walks contiguous element ranges (same rows, same query) and a
@@ -657,7 +739,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
       const uint32_t rlo = __ldg(a.tile_row + tile), rhi = __ldg(a.tile_row + tile + 1);
       const uint64_t t = tb + threadIdx.x;
       const bool valid = t < te;
-      bool ok = false, fin = false, fused = false;
+      bool ok = false, fin = false, fused = false, ftail = false;
       uint32_t r = 0, x = 0, q = 0;
       if (valid) {
         r = find_row(a.woff, rlo, rhi, t);
@@ -686,13 +768,12 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
           if (c == ci) continue;
           const uint32_t cs = P.cons[i][c];
           const uint32_t y = a.in.col[cs & 0xFF][r];
-          uint32_t s, en;
-          slice_of(g, cs >> 8, y, lab, s, en);
-          ok = contains(g.adj[cs >> 8], s, en, x);
+          ok = in_slice(g, cs >> 8, y, lab, x);
         }
         if (ok && ((P.selfloop_mask >> i) & 1u)) ok = has_self(g, x);
         fin = (i + 1 == P.k);
         fused = !fin && a.count_mode && (i + 2 == P.k) && P.last_o1;
+        ftail = a.tail_dense && P.tail2 && i + 3 == P.k;
         // Filters prune positions whose survivors are extended further; the
         // position before a last position counted in closed form is not
         // filtered (the closed form already yields 0 for hopeless candidates).
@@ -700,13 +781,28 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
           ok = pass_filters(g, P, i, x, a.filters);
         if (ok) {
           if (q != cnt_q) {
-            acc_flush(a, cnt_q, i, cnt, s1, sk);
-            cnt = s1 = sk = 0;
+            acc_flush(a, cnt_q, i, cnt, s1, sk, s2);
+            cnt = s1 = sk = s2 = 0;
             cnt_q = q;
           }
           s1 += 1;
           if (fin) {
             if (a.count_mode) cnt += 1;
+          } else if (ftail) {
+            // The prefix ending in x has length k-2: its two-position pendant
+            // tail is counted here from the dense aggregates, not stored.
+            const uint32_t mp = P.tail_p == i ? x : a.in.col[P.tail_p][r];
+            uint32_t ts, te;
+            slice_of(g, P.tail_da, mp, P.label[P.k - 2], ts, te);
+            const uint64_t idx = a.tkeys[P.tail_kid].base + __ldg(g.bucket_pos + mp);
+            unsigned long long tc, tp, td;
+            tail_close(a, P, [&](uint32_t j) { return j == i ? x : a.in.col[j][r]; }, mp, ts, te,
+                       (long long)a.tdA[idx], (long long)a.tdAD[idx], tc, tp, td);
+            cnt += tc;
+            sk += tc;
+            s2 += tp;
+            bal += 8ull + 4ull * (te - ts) + 8ull * tp + 4ull * td;
+            balc += 8ull + 4ull * (te - ts) + 8ull * tp;
           } else if (fused) {
             const uint32_t kl = P.k - 1;
             const uint32_t cs = P.cons[kl][0];
@@ -723,7 +819,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
                 c1 -= 1;
               } else {
                 const uint32_t mj = j == i ? x : a.in.col[j][r];
-                c1 -= contains(g.adj[dir], s, en, mj) ? 1ull : 0ull;
+                c1 -= in_slice_se(g, dir, y, s, en, mj) ? 1ull : 0ull;
               }
             }
             sk += c1;
@@ -736,7 +832,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
       // query) contiguous in the next table.
       // Launches without an output table (last or closed-form positions) skip
       // the reservation and its barriers.
-      const bool wr = ok && !fin && !fused;
+      const bool wr = ok && !fin && !fused && !ftail;
       if (a.out_cap) {
         const uint32_t wm = __ballot_sync(FULL, wr);
         if (lane == 0) s_wcnt[threadIdx.x >> 5] = __popc(wm);
@@ -789,9 +885,9 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
       if (a.out_cap) __syncthreads();  // s_wcnt / s_wbase are reused by the next tile
     }
     // Once per grab: fold the per-thread counts of a warp that holds one query.
-    acc_flush_warp(a, cnt_q, i, cnt, s1, sk, false);
+    acc_flush_warp(a, cnt_q, i, cnt, s1, sk, s2, false);
   }  // grab loop
-  acc_flush_warp(a, cnt_q, i, cnt, s1, sk, true);
+  acc_flush_warp(a, cnt_q, i, cnt, s1, sk, s2, true);
   bal = warp_sum(bal);
   balc = warp_sum(balc);
   if (lane == 0 && (bal | balc)) {
@@ -969,11 +1065,6 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
   MG_CK(cudaMemsetAsync(ws->ctr, 0, C_NUM * 8, st));
   MG_CK(cudaEventRecord(ws->ev0, st));
 
-  // writes[l]: some query can append rows to the level-(l+1) table.
-  bool writes[MAXK] = {};
-  for (uint32_t l = 0; l < kmax; ++l)
-    for (auto& p : plans)
-      if (p.k > l + 1 && !(count_mode && p.k == l + 2 && p.last_o1)) writes[l] = true;
 
   StepArgs a;
   std::memset(&a, 0, sizeof(a));
@@ -1015,23 +1106,60 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
   // memo table of two-hop aggregates, shared by every query of the call.
   uint32_t tail_levels = 0;
   uint64_t hsize_used = 0, keyspace = 0;
+  bool dense = false;
   if (count_mode && o.no_tail != 1) {
+    // Tail keys (da, la, db, lb, lp): the aggregates depend on the label of
+    // m_p only through which vertices occur, so keys with different lp are
+    // kept apart for the dense layout.
     std::vector<TailKey> keys;
-    std::vector<uint64_t> key_lp;  // (kid << 32 | label of m_p): key space per pair
     for (PlanDev& p : plans) {
       if (!p.tail2) continue;
-      const TailKey tk{p.tail_da, p.label[p.k - 2], p.tail_db, p.label[p.k - 1]};
+      TailKey tk{p.tail_da, p.label[p.k - 2], p.tail_db, p.label[p.k - 1], p.label[p.tail_p], 0, 0};
       uint32_t kid = 0;
       while (kid < keys.size() && std::memcmp(&keys[kid], &tk, sizeof(tk)) != 0) ++kid;
-      if (kid == keys.size()) keys.push_back(tk);
+      if (kid == keys.size()) {
+        keys.push_back(tk);
+        keyspace += dg->h_bucket_off[tk.lp + 1] - dg->h_bucket_off[tk.lp];
+      }
       p.tail_kid = kid;
       tail_levels |= 1u << (p.k - 2);
-      const uint32_t lp = p.label[p.tail_p];
-      const uint64_t kl = (uint64_t(kid) << 32) | lp;
-      if (std::find(key_lp.begin(), key_lp.end(), kl) == key_lp.end()) {
-        key_lp.push_back(kl);
-        keyspace += dg->h_bucket_off[lp + 1] - dg->h_bucket_off[lp];
+    }
+    // Dense aggregates over whole buckets when there are few keys: each
+    // costs one pass over the bucket's la-slices, and the tail is then
+    // counted while expanding position k-3 (its rows are never stored).
+    // Otherwise aggregates are memoised for the keys that occur.
+    dense = !keys.empty() && keys.size() <= 8 && keyspace <= (1ull << 27);
+    if (dense) {
+      uint64_t base = 0;
+      for (TailKey& tk : keys) {
+        tk.base = base;
+        base += dg->h_bucket_off[tk.lp + 1] - dg->h_bucket_off[tk.lp];
       }
+      if (ws->td_cap < base) {
+        if ((rc = ws_alloc(ws, (void**)&ws->tdA, base * 8))) return rc;
+        if ((rc = ws_alloc(ws, (void**)&ws->tdAD, base * 8))) return rc;
+        ws->td_cap = base;
+      }
+      if (ws->tkeys_cap < keys.size()) {
+        if ((rc = ws_alloc(ws, (void**)&ws->tkeys, keys.size() * sizeof(TailKey)))) return rc;
+        ws->tkeys_cap = uint32_t(keys.size());
+      }
+      MG_CK(cudaMemcpyAsync(ws->tkeys, keys.data(), keys.size() * sizeof(TailKey),
+                            cudaMemcpyHostToDevice, st));
+      MG_CK(cudaMemcpyAsync(ws->plans, plans.data(), nq * sizeof(PlanDev), cudaMemcpyHostToDevice,
+                            st));
+      for (const TailKey& tk : keys) {
+        const uint32_t nb = dg->h_bucket_off[tk.lp + 1] - dg->h_bucket_off[tk.lp];
+        if (!nb) continue;
+        k_tail_dense<<<grid_for(uint64_t(nb) * 32, 256, sms * 16), 256, 0, st>>>(
+            dg->g, tk, nb, ws->tdA, ws->tdAD);
+        res->launches++;
+      }
+      a.tail_dense = 1;
+      a.tdA = ws->tdA;
+      a.tdAD = ws->tdAD;
+      a.tkeys = ws->tkeys;
+      tail_levels = 0;
     }
     if (tail_levels) {
       // Table size: twice the distinct keys that can occur (vertices of the
@@ -1063,6 +1191,14 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
       a.tkeys = ws->tkeys;
     }
   }
+  // writes[l]: some query can append rows to the level-(l+1) table.
+  bool writes[MAXK] = {};
+  for (uint32_t l = 0; l < kmax; ++l)
+    for (auto& p : plans)
+      if (p.k > l + 1 && !(count_mode && p.k == l + 2 && p.last_o1) &&
+          !(dense && p.tail2 && p.k == l + 3))
+        writes[l] = true;
+
   uint64_t memo_fill = 0;  // slots used in the memo table
   auto launch_work_scan = [&](int l) -> int {
     a.tail_on = (tail_levels >> l) & 1u;

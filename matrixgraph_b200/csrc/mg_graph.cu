@@ -9,6 +9,7 @@
 // kernel_woj_subsio.cu:385-446) and label buckets (the level-0 candidate
 // ranges).
 #include <algorithm>
+#include <functional>
 #include <cstdlib>
 #include <cstring>
 #include <thread>
@@ -249,6 +250,76 @@ inline unsigned grid_for(uint64_t items, unsigned block, unsigned cap) {
 
 }  // namespace
 
+// Hub bitmaps: block h sets the bits of hub h's whole d-adjacency (the
+// label-ordered list of vertex y spans [loff[y*L], loff[(y+1)*L])).
+__global__ void __launch_bounds__(256) k_hub_bits(const uint32_t* __restrict__ adj,
+                                                  const uint32_t* __restrict__ loff, uint32_t L,
+                                                  const uint32_t* __restrict__ hub_vid,
+                                                  uint32_t words, uint32_t* bits) {
+  const uint32_t y = hub_vid[blockIdx.x];
+  const uint32_t s = loff[uint64_t(y) * L], e = loff[uint64_t(y + 1) * L];
+  uint32_t* row = bits + uint64_t(blockIdx.x) * words;
+  for (uint32_t j = s + threadIdx.x; j < e; j += blockDim.x) {
+    const uint32_t x = adj[j];
+    atomicOr(row + (x >> 5), 1u << (x & 31));
+  }
+}
+
+// Selects the hubs of direction d (decreasing degree within the byte budget,
+// ties at the cut all in or all out) and builds their bitmaps.
+static int build_hubs(DevGraph* dg, int d, const std::vector<uint32_t>& deg, uint64_t budget,
+                      uint32_t min_degree) {
+  const uint32_t n = dg->g.n;
+  const uint32_t words = ((n + 31) / 32 + 3) & ~3u;  // rows start on 16-byte boundaries
+  const uint64_t row_bytes = uint64_t(words) * 4;
+  uint64_t cap = std::min<uint64_t>(budget / row_bytes, NO_HUB);
+  if (cap == 0) return MG_OK;
+  std::vector<uint32_t> cand;
+  for (uint32_t v = 0; v < n; ++v)
+    if (deg[v] >= min_degree) cand.push_back(v);
+  if (cand.empty()) return MG_OK;
+  uint32_t cut = min_degree;
+  if (cand.size() > cap) {
+    std::vector<uint32_t> dv(cand.size());
+    for (size_t i = 0; i < cand.size(); ++i) dv[i] = deg[cand[i]];
+    std::nth_element(dv.begin(), dv.begin() + (cap - 1), dv.end(), std::greater<uint32_t>());
+    cut = dv[cap - 1];  // the cap-th largest degree
+    uint64_t at_or_above = 0;
+    for (uint32_t x : dv) at_or_above += x >= cut;
+    if (at_or_above > cap) ++cut;  // ties at the cut would overflow: leave them out
+  }
+  std::vector<uint32_t> hub_vid;
+  std::vector<uint16_t> slot(n, NO_HUB);
+  for (uint32_t v : cand)
+    if (deg[v] >= cut) {
+      slot[v] = uint16_t(hub_vid.size());
+      hub_vid.push_back(v);
+    }
+  if (hub_vid.empty()) return MG_OK;
+  cudaStream_t st = dg->stream;
+  uint16_t* d_slot;
+  uint32_t *d_bits, *d_vid;
+  int rc;
+  if ((rc = dev_alloc(dg, (void**)&d_slot, uint64_t(n) * 2))) return rc;
+  if ((rc = dev_alloc(dg, (void**)&d_bits, hub_vid.size() * row_bytes))) return rc;
+  MG_CK(cudaMallocAsync((void**)&d_vid, hub_vid.size() * 4, st));
+  MG_CK(cudaMemcpyAsync(d_slot, slot.data(), uint64_t(n) * 2, cudaMemcpyHostToDevice, st));
+  MG_CK(cudaMemcpyAsync(d_vid, hub_vid.data(), hub_vid.size() * 4, cudaMemcpyHostToDevice, st));
+  MG_CK(cudaMemsetAsync(d_bits, 0, hub_vid.size() * row_bytes, st));
+  k_hub_bits<<<unsigned(hub_vid.size()), 256, 0, st>>>(dg->g.adj[d], dg->g.loff[d], dg->g.L,
+                                                      d_vid, words, d_bits);
+  MG_CK(cudaGetLastError());
+  cudaFreeAsync(d_vid, st);
+  MG_CK(cudaStreamSynchronize(st));
+  dg->g.hub_slot[d] = d_slot;
+  dg->g.hub_bits[d] = d_bits;
+  dg->g.hub_words = words;
+  dg->info.hubs += uint32_t(hub_vid.size());
+  dg->info.hub_min_degree = cut;
+  dg->info.hub_bytes += hub_vid.size() * row_bytes;
+  return MG_OK;
+}
+
 // Builds adjacency + slices for one direction from raw host arrays.
 static int build_direction(DevGraph* dg, int d, const uint32_t* h_off, const uint32_t* h_adj,
                            uint32_t m, const uint32_t* d_g2l, uint32_t max_vid,
@@ -326,7 +397,7 @@ static int build_direction(DevGraph* dg, int d, const uint32_t* h_off, const uin
   return MG_OK;
 }
 
-static int upload(const mg_csr_view* v, int device, DevGraph* dg) {
+static int upload(const mg_csr_view* v, int device, const mg_upload_opts& uo, DevGraph* dg) {
   int rc = validate_csr_view(v);
   if (rc) return rc;
   if (v->n == 0) return set_error(MG_E_ARG, "empty data graph");
@@ -371,15 +442,19 @@ static int upload(const mg_csr_view* v, int device, DevGraph* dg) {
   dg->stats.label_count = cnt;
   dg->h_bucket_off.assign(L + 1, 0);
   for (uint32_t l = 0; l < L; ++l) dg->h_bucket_off[l + 1] = dg->h_bucket_off[l] + uint32_t(cnt[l]);
-  std::vector<uint32_t> bvid(n);
+  std::vector<uint32_t> bvid(n), bpos(n);
   {
     std::vector<uint32_t> cur(dg->h_bucket_off.begin(), dg->h_bucket_off.end() - 1);
-    for (uint32_t i = 0; i < n; ++i) bvid[cur[lab[i]]++] = i;
+    for (uint32_t i = 0; i < n; ++i) {
+      bpos[i] = cur[lab[i]] - dg->h_bucket_off[lab[i]];
+      bvid[cur[lab[i]]++] = i;
+    }
   }
-  uint32_t *d_label, *d_boff, *d_bvid, *d_self, *d_gid, *d_err;
+  uint32_t *d_label, *d_boff, *d_bvid, *d_bpos, *d_self, *d_gid, *d_err;
   if ((rc = dev_alloc(dg, (void**)&d_label, uint64_t(n) * 4))) return rc;
   if ((rc = dev_alloc(dg, (void**)&d_boff, uint64_t(L + 1) * 4))) return rc;
   if ((rc = dev_alloc(dg, (void**)&d_bvid, uint64_t(n) * 4))) return rc;
+  if ((rc = dev_alloc(dg, (void**)&d_bpos, uint64_t(n) * 4))) return rc;
   if ((rc = dev_alloc(dg, (void**)&d_self, uint64_t((n + 31) / 32) * 4))) return rc;
   if ((rc = dev_alloc(dg, (void**)&d_gid, uint64_t(n) * 4))) return rc;
   if ((rc = dev_alloc(dg, (void**)&d_err, 16))) return rc;
@@ -387,12 +462,14 @@ static int upload(const mg_csr_view* v, int device, DevGraph* dg) {
   MG_CK(cudaMemcpyAsync(d_boff, dg->h_bucket_off.data(), uint64_t(L + 1) * 4,
                         cudaMemcpyHostToDevice, st));
   MG_CK(cudaMemcpyAsync(d_bvid, bvid.data(), uint64_t(n) * 4, cudaMemcpyHostToDevice, st));
+  MG_CK(cudaMemcpyAsync(d_bpos, bpos.data(), uint64_t(n) * 4, cudaMemcpyHostToDevice, st));
   MG_CK(cudaMemcpyAsync(d_gid, v->globalid, uint64_t(n) * 4, cudaMemcpyHostToDevice, st));
   MG_CK(cudaMemsetAsync(d_self, 0, uint64_t((n + 31) / 32) * 4, st));
   MG_CK(cudaMemsetAsync(d_err, 0, 16, st));
   dg->g.label = d_label;
   dg->g.bucket_off = d_boff;
   dg->g.bucket_vid = d_bvid;
+  dg->g.bucket_pos = d_bpos;
   dg->g.selfbits = d_self;
   dg->g.globalid = d_gid;
 
@@ -429,11 +506,23 @@ static int upload(const mg_csr_view* v, int device, DevGraph* dg) {
   MG_CK(cudaStreamSynchronize(st));
   if (err & ERR_RANGE) return set_error(MG_E_FORMAT, "vertex id outside [0, max_vid] or unknown");
   // Maximum degree (host reduction over the reference outdeg is not trusted:
-  // read the distinct-neighbour degrees back).
-  {
+  // read the distinct-neighbour degrees back), then the hub bitmaps.
+  uint64_t budget = uo.hub_bytes;
+  if (budget == MG_HUB_AUTO) {
+    size_t free_b = 0, total_b = 0;
+    MG_CK(cudaMemGetInfo(&free_b, &total_b));
+    budget = std::min<uint64_t>(1ull << 30, free_b / 8);
+  }
+  const uint32_t min_degree = uo.hub_min_degree ? uo.hub_min_degree : 128u;
+  for (int d = 0; d < (sym ? 1 : 2); ++d) {
     std::vector<uint32_t> h(n);
-    MG_CK(cudaMemcpy(h.data(), dg->g.deg[0], uint64_t(n) * 4, cudaMemcpyDeviceToHost));
-    dg->info.max_degree = *std::max_element(h.begin(), h.end());
+    MG_CK(cudaMemcpy(h.data(), dg->g.deg[d], uint64_t(n) * 4, cudaMemcpyDeviceToHost));
+    if (d == 0) dg->info.max_degree = *std::max_element(h.begin(), h.end());
+    if (budget && (rc = build_hubs(dg, d, h, sym ? budget : budget / 2, min_degree))) return rc;
+  }
+  if (sym) {
+    dg->g.hub_slot[1] = dg->g.hub_slot[0];
+    dg->g.hub_bits[1] = dg->g.hub_bits[0];
   }
   return MG_OK;
 }
@@ -515,15 +604,23 @@ int env_or_current_device(int* dev) {
 extern "C" {
 
 int mg_graph_upload(const mg_csr_view* g, int device, void** dgraph) {
+  return mg_graph_upload_ex(g, device, nullptr, dgraph);
+}
+
+int mg_graph_upload_ex(const mg_csr_view* g, int device, const mg_upload_opts* opts,
+                       void** dgraph) {
   mg::clear_error();
   if (!g || !dgraph) return mg::set_error(MG_E_ARG, "null argument");
+  mg_upload_opts uo{MG_HUB_AUTO, 0, 0};
+  if (opts) uo = *opts;
+  if (uo._reserved) return mg::set_error(MG_E_ARG, "reserved upload option must be 0");
   auto* dg = new (std::nothrow) mg::DevGraph();
   if (!dg) return mg::set_error(MG_E_OOM, "host allocation failed");
   int prev = 0;
   cudaGetDevice(&prev);
   int rc;
   try {
-    rc = mg::upload(g, device, dg);
+    rc = mg::upload(g, device, uo, dg);
   } catch (const std::bad_alloc&) {
     rc = mg::set_error(MG_E_OOM, "host allocation failed");
   }

@@ -76,9 +76,14 @@ def plan_order(q: CSRGraph, order="reference", graph: "DeviceGraph | None" = Non
 class DeviceGraph:
     """A data graph resident on one GPU with its derived indices."""
 
-    def __init__(self, g: CSRGraph, device: int = 0):
+    def __init__(self, g: CSRGraph, device: int = 0, hub_bytes: int | None = None,
+                 hub_min_degree: int = 0):
+        """Uploads ``g``; ``hub_bytes`` caps the hub bitmaps (None: the library
+        default, 0: none), ``hub_min_degree`` is the smallest hub degree."""
         h = C.c_void_p()
-        L.check(L.lib.mg_graph_upload(C.byref(g.view), device, C.byref(h)))
+        uo = L.UploadOpts(L.MG_HUB_AUTO if hub_bytes is None else int(hub_bytes),
+                          int(hub_min_degree), 0)
+        L.check(L.lib.mg_graph_upload_ex(C.byref(g.view), device, C.byref(uo), C.byref(h)))
         self.handle = h.value
         self.device = device
 

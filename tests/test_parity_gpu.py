@@ -345,3 +345,38 @@ def test_root_step_partitions_and_matches_oracle():
             assert len(rows) == O.count(og, oq, root_range=(2, 2 ** 63), root_step=4)["count"]
     finally:
         dg.free()
+
+
+@pytest.mark.parametrize("directed", [False, True])
+def test_hub_bitmaps_never_change_results(directed):
+    """Counts, P_i and emitted rows are identical whether slice probes go to
+    hub bitmaps (every vertex a hub, a budget that cuts through the degree
+    order) or to binary search only."""
+    rng = np.random.default_rng(11 if directed else 12)
+    n = 400
+    edges, labels = random_graph(rng, n, 0.03, 3, directed=directed, self_loops=True)
+    g = graph(n, edges, labels, symmetric=not directed)
+    handles = {"none": mg.DeviceGraph(g, hub_bytes=0),
+               "all": mg.DeviceGraph(g, hub_bytes=1 << 30, hub_min_degree=1),
+               "cut": mg.DeviceGraph(g, hub_bytes=7 * 64, hub_min_degree=1)}
+    try:
+        assert handles["none"].info["hubs"] == 0
+        assert handles["all"].info["hubs"] > 0 and handles["cut"].info["hubs"] > 0
+        assert handles["cut"].info["hubs"] <= 7 * (1 if not directed else 1)
+        for t in range(12):
+            k = 3 + t % 4
+            qe, ql = random_query(rng, k, 0.4, 3, directed=directed)
+            q = mg.CSRGraph.query(k, qe, ql, directed=directed)
+            want = oracle_count(g, q)
+            for name, dg in handles.items():
+                for no_tail in (0, 1):
+                    c, st = dg.count(q, stats=True, no_tail=no_tail)
+                    assert c == want["count"], (name, t, no_tail)
+                    assert st["level_rows"] == want["level_rows"], (name, t, no_tail)
+            if want["count"] <= 20000:
+                rows = oracle_rows(g, q)
+                for name, dg in handles.items():
+                    assert np.array_equal(dg.emit(q), rows), (name, t)
+    finally:
+        for dg in handles.values():
+            dg.free()
