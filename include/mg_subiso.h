@@ -152,7 +152,7 @@ typedef struct mg_graph_info {
  * (ties at the cut are all taken or all left out).                        */
 #define MG_HUB_AUTO (~(uint64_t)0)
 typedef struct mg_upload_opts {
-  uint64_t hub_bytes;        /* MG_HUB_AUTO: min(1 GiB, free device memory/8);
+  uint64_t hub_bytes;        /* MG_HUB_AUTO: min(4 GiB, free device memory/8);
                                 0: no hub bitmaps                            */
   uint32_t hub_min_degree;   /* smallest degree of a hub; 0 = 128             */
   uint32_t _reserved;        /* must be 0                                    */

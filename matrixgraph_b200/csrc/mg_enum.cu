@@ -711,7 +711,17 @@ __global__ void __launch_bounds__(256) k_tile_rows(const uint64_t* __restrict__ 
   }
 }
 
+// Launch shapes of the expand kernel, fixed at compile time so a launch
+// carries only the code (and registers) of the paths its rows can take.
+enum : int {
+  X_WRITE = 1,  // survivors are appended to the next level table
+  X_EMIT = 2,   // complete matches are written as rows (emit mode)
+  X_FUSED = 4,  // the last position (one backward slice) is closed in place
+  X_TAIL = 8,   // a two-position pendant tail is closed from dense aggregates
+};
+
 // Expand kernel: one element (row, driving entry) per thread.
+template <int MODE>
 __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
   const uint32_t i = a.level;
   const GraphDev& g = a.g;
@@ -772,8 +782,9 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
         }
         if (ok && ((P.selfloop_mask >> i) & 1u)) ok = has_self(g, x);
         fin = (i + 1 == P.k);
-        fused = !fin && a.count_mode && (i + 2 == P.k) && P.last_o1;
-        ftail = a.tail_dense && P.tail2 && i + 3 == P.k;
+        if constexpr ((MODE & X_FUSED) != 0)
+          fused = !fin && a.count_mode && (i + 2 == P.k) && P.last_o1;
+        if constexpr ((MODE & X_TAIL) != 0) ftail = a.tail_dense && P.tail2 && i + 3 == P.k;
         // Filters prune positions whose survivors are extended further; the
         // position before a last position counted in closed form is not
         // filtered (the closed form already yields 0 for hopeless candidates).
@@ -788,7 +799,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
           s1 += 1;
           if (fin) {
             if (a.count_mode) cnt += 1;
-          } else if (ftail) {
+          } else if ((MODE & X_TAIL) && ftail) {
             // The prefix ending in x has length k-2: its two-position pendant
             // tail is counted here from the dense aggregates, not stored.
             const uint32_t mp = P.tail_p == i ? x : a.in.col[P.tail_p][r];
@@ -803,7 +814,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
             s2 += tp;
             bal += 8ull + 4ull * (te - ts) + 8ull * tp + 4ull * td;
             balc += 8ull + 4ull * (te - ts) + 8ull * tp;
-          } else if (fused) {
+          } else if ((MODE & X_FUSED) && fused) {
             const uint32_t kl = P.k - 1;
             const uint32_t cs = P.cons[kl][0];
             const uint32_t pos = cs & 0xFF, dir = cs >> 8;
@@ -833,7 +844,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
       // Launches without an output table (last or closed-form positions) skip
       // the reservation and its barriers.
       const bool wr = ok && !fin && !fused && !ftail;
-      if (a.out_cap) {
+      if constexpr ((MODE & X_WRITE) != 0) {
         const uint32_t wm = __ballot_sync(FULL, wr);
         if (lane == 0) s_wcnt[threadIdx.x >> 5] = __popc(wm);
         __syncthreads();
@@ -863,6 +874,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
         atomicOr(&a.ctr[C_ERR], (unsigned long long)ERR_OVERFLOW);  // no table to append to
       }
       // Emit mode: complete matches as rows in query-vertex order.
+      if constexpr ((MODE & X_EMIT) != 0) {
       const bool em = ok && fin && !a.count_mode;
       const uint32_t emm = __ballot_sync(FULL, em);
       if (emm) {
@@ -882,7 +894,8 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
           }
         }
       }
-      if (a.out_cap) __syncthreads();  // s_wcnt / s_wbase are reused by the next tile
+      }  // X_EMIT
+      if constexpr ((MODE & X_WRITE) != 0) __syncthreads();  // s_wcnt / s_wbase reused next tile
     }
     // Once per grab: fold the per-thread counts of a warp that holds one query.
     acc_flush_warp(a, cnt_q, i, cnt, s1, sk, s2, false);
@@ -1030,6 +1043,33 @@ struct RunResult {
 static inline unsigned grid_for(uint64_t items, unsigned block, unsigned cap) {
   uint64_t g = (items + block - 1) / block;
   return unsigned(std::max<uint64_t>(1, std::min<uint64_t>(g, cap)));
+}
+
+// Launches the expand kernel specialised for what the rows of level `lvl`
+// can need: a write when the level writes a table, emit rows in emit mode,
+// in-place closing of a last position or of a pendant tail when a plan has
+// one right after this position.
+static void launch_expand(const StepArgs& a, const PlanDev* plans, uint32_t nplans,
+                          bool count_mode, bool writes, unsigned grid, cudaStream_t st) {
+  const uint32_t i = a.level;
+  bool fused = false, tail = false, emit = false;
+  for (uint32_t pi = 0; pi < nplans; ++pi) {
+    const PlanDev& p = plans[pi];
+    if (count_mode && p.k == i + 2 && p.last_o1) fused = true;
+    if (a.tail_dense && p.tail2 && p.k == i + 3) tail = true;
+    if (!count_mode && p.k == i + 1) emit = true;
+  }
+  const int mode = (writes ? X_WRITE : 0) | (emit ? X_EMIT : 0) | (fused ? X_FUSED : 0) |
+                   (tail ? X_TAIL : 0);
+  switch (mode) {
+#define MG_X(m) \
+  case m:       \
+    k_expand<m><<<grid, EXPAND_BLOCK, 0, st>>>(a); \
+    break;
+    MG_X(0) MG_X(1) MG_X(2) MG_X(3) MG_X(4) MG_X(5) MG_X(6) MG_X(7)
+    MG_X(8) MG_X(9) MG_X(10) MG_X(11) MG_X(12) MG_X(13) MG_X(14) MG_X(15)
+#undef MG_X
+  }
 }
 
 static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
@@ -1283,7 +1323,8 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
         k_tile_rows<<<grid_for(uint64_t(ntiles) + 1, 256, sms * 16), 256, 0, st>>>(
             ws->woff[lvl], R[lvl], s0, s1, ntiles, ws->tile_row);
         MG_CK(cudaMemsetAsync(ws->ctr + C_TILE, 0, 8, st));
-        k_expand<<<grid_for(s1 - s0, EXPAND_BLOCK, sms * 8), EXPAND_BLOCK, 0, st>>>(a);
+        launch_expand(a, plans.data(), nq, count_mode, writes[lvl],
+                      grid_for(s1 - s0, EXPAND_BLOCK, sms * 8), st);
         res->launches += 2;
       }
       res->chunks++;
@@ -1875,7 +1916,8 @@ int noalloc_count(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint6
         k_tile_rows<<<grid_for(uint64_t(ntiles) + 1, 256, sms * 16), 256, 0, st>>>(
             L.woff[lvl], R[lvl], s0, s1, ntiles, L.tile_row);
         MG_CK(cudaMemsetAsync(L.ctr + C_TILE, 0, 8, st));
-        k_expand<<<grid_for(s1 - s0, EXPAND_BLOCK, sms * 8), EXPAND_BLOCK, 0, st>>>(a);
+        launch_expand(a, &P, 1, true, writes[lvl],
+                      grid_for(s1 - s0, EXPAND_BLOCK, sms * 8), st);
       }
       MG_CK(cudaGetLastError());
       cur[lvl] = t1;

@@ -511,7 +511,7 @@ static int upload(const mg_csr_view* v, int device, const mg_upload_opts& uo, De
   if (budget == MG_HUB_AUTO) {
     size_t free_b = 0, total_b = 0;
     MG_CK(cudaMemGetInfo(&free_b, &total_b));
-    budget = std::min<uint64_t>(1ull << 30, free_b / 8);
+    budget = std::min<uint64_t>(4ull << 30, free_b / 8);
   }
   const uint32_t min_degree = uo.hub_min_degree ? uo.hub_min_degree : 128u;
   for (int d = 0; d < (sym ? 1 : 2); ++d) {
