@@ -58,7 +58,7 @@ class CsrView(C.Structure):
 class Opts(C.Structure):
     _fields_ = [("order", C.c_int32), ("filters", C.c_uint32), ("given_order", P32),
                 ("model", C.c_void_p), ("chunk_rows", C.c_uint64), ("grab", C.c_uint32),
-                ("root_step", C.c_uint32), ("_reserved0", C.c_uint32),
+                ("root_step", C.c_uint32), ("probe_min", C.c_uint32),
                 ("_reserved1", C.c_uint32), ("mem_budget_bytes", C.c_uint64),
                 ("root_begin", C.c_uint64), ("root_end", C.c_uint64),
                 ("no_tail", C.c_uint32), ("_reserved", C.c_uint32),

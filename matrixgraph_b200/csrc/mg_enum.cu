@@ -107,6 +107,7 @@ static int ws_alloc(Workspace* ws, void** p, size_t bytes) {
 }
 
 constexpr uint64_t kDefaultCap = 1ull << 24;
+constexpr uint32_t kProbeMin = 32;  // default shortest hub slice probed by bitmap
 constexpr int SCAN_TILE = 4096;
 constexpr int EXPAND_BLOCK = 256;                 // elements per expand tile
 constexpr uint64_t kSegment = 1ull << 26;         // elements per expand launch
@@ -191,6 +192,7 @@ struct StepArgs {
   uint64_t emit_cap;
   uint64_t root_begin, root_end;  // level-0 candidate range (root_end 0: all)
   uint32_t root_step;             // level-0 stride inside the range (>= 1)
+  uint32_t probe_min;             // shortest hub slice probed in the hub bitmap
   const uint32_t* tile_row;        // first row of each tile of [t0, t1)
   // Pendant tails counted in closed form (tail_on): memo table of aggregates.
   uint32_t grab;   // expand tiles taken per work-queue grab
@@ -233,31 +235,36 @@ __device__ __forceinline__ void slice_of(const GraphDev& g, uint32_t dir, uint32
   e = __ldg(p + 1);
 }
 
+// Probe strategy: a slice of a hub with at least `pmin` entries is probed in
+// the hub's bitmap (one load, but a random sector of a row that may not sit
+// in L2); shorter slices and non-hubs by binary search (a few loads that
+// usually hit L1, since the elements of one row probe the same slice).
+__device__ __forceinline__ bool hub_bit(const GraphDev& g, uint32_t d, uint16_t h, uint32_t x) {
+  return (__ldg(g.hub_bits[d] + uint64_t(h) * g.hub_words + (x >> 5)) >> (x & 31)) & 1u;
+}
+
 // x in the d-adjacency of y, where x is known to carry the label of the slice
-// [s, e) of y being asked about: a hub's bitmap answers with one load, any
-// other vertex by binary search in the slice.
+// [s, e) of y being asked about.
 __device__ __forceinline__ bool in_slice_se(const GraphDev& g, uint32_t d, uint32_t y, uint32_t s,
-                                            uint32_t e, uint32_t x) {
-  if (g.hub_slot[d]) {
+                                            uint32_t e, uint32_t x, uint32_t pmin) {
+  if (g.hub_slot[d] && e - s >= pmin) {
     const uint16_t h = __ldg(g.hub_slot[d] + y);
-    if (h != NO_HUB)
-      return (__ldg(g.hub_bits[d] + uint64_t(h) * g.hub_words + (x >> 5)) >> (x & 31)) & 1u;
+    if (h != NO_HUB) return hub_bit(g, d, h, x);
   }
   return contains(g.adj[d], s, e, x);
 }
 
-// x (labelled lab) in the label-lab slice of y's d-adjacency; a hub needs no
-// slice offsets at all.
+// x (labelled lab) in the label-lab slice of y's d-adjacency; with pmin <= 1
+// a hub needs no slice offsets at all.
 __device__ __forceinline__ bool in_slice(const GraphDev& g, uint32_t d, uint32_t y, uint32_t lab,
-                                         uint32_t x) {
-  if (g.hub_slot[d]) {
+                                         uint32_t x, uint32_t pmin) {
+  if (g.hub_slot[d] && pmin <= 1) {
     const uint16_t h = __ldg(g.hub_slot[d] + y);
-    if (h != NO_HUB)
-      return (__ldg(g.hub_bits[d] + uint64_t(h) * g.hub_words + (x >> 5)) >> (x & 31)) & 1u;
+    if (h != NO_HUB) return hub_bit(g, d, h, x);
   }
   uint32_t s, e;
   slice_of(g, d, y, lab, s, e);
-  return contains(g.adj[d], s, e, x);
+  return in_slice_se(g, d, y, s, e, x, pmin);
 }
 
 __device__ __forceinline__ bool pass_filters(const GraphDev& g, const PlanDev& P, uint32_t i,
@@ -473,7 +480,7 @@ __device__ __forceinline__ void tail_close(const StepArgs& a, const PlanDev& P, 
   for (uint32_t mi = P.tail_Ia; mi; mi &= mi - 1) {
     const uint32_t i2 = __ffs(mi) - 1;
     const uint32_t x = col(i2);
-    if (!in_slice_se(g, da, mp, s, e, x)) continue;
+    if (!in_slice_se(g, da, mp, s, e, x, a.probe_min)) continue;
     inS += 1;
     uint32_t xs, xe;
     slice_of(g, db, x, lb, xs, xe);
@@ -482,7 +489,7 @@ __device__ __forceinline__ void tail_close(const StepArgs& a, const PlanDev& P, 
     if (la == lb && has_self(g, x)) cx -= 1;
     for (uint32_t mj = P.tail_J; mj; mj &= mj - 1) {
       const uint32_t j = __ffs(mj) - 1;
-      if (in_slice_se(g, db, x, xs, xe, col(j))) cx -= 1;
+      if (in_slice_se(g, db, x, xs, xe, col(j), a.probe_min)) cx -= 1;
     }
     c -= cx;
   }
@@ -778,7 +785,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
           if (c == ci) continue;
           const uint32_t cs = P.cons[i][c];
           const uint32_t y = a.in.col[cs & 0xFF][r];
-          ok = in_slice(g, cs >> 8, y, lab, x);
+          ok = in_slice(g, cs >> 8, y, lab, x, a.probe_min);
         }
         if (ok && ((P.selfloop_mask >> i) & 1u)) ok = has_self(g, x);
         fin = (i + 1 == P.k);
@@ -830,7 +837,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
                 c1 -= 1;
               } else {
                 const uint32_t mj = j == i ? x : a.in.col[j][r];
-                c1 -= in_slice_se(g, dir, y, s, en, mj) ? 1ull : 0ull;
+                c1 -= in_slice_se(g, dir, y, s, en, mj, a.probe_min) ? 1ull : 0ull;
               }
             }
             sk += c1;
@@ -1125,6 +1132,7 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
     a.emit_cap = emit->cap;
   }
   a.root_step = o.root_step > 1 ? o.root_step : 1u;
+  a.probe_min = o.probe_min ? o.probe_min : kProbeMin;
   if (o.root_end || a.root_step > 1) {
     a.root_begin = o.root_begin;
     a.root_end = o.root_end ? o.root_end : ~0ull;
@@ -1457,7 +1465,7 @@ static mg_opts resolve_opts(const mg_opts* o) {
 
 // Checks that do not depend on the query or the graph.
 static int check_opts(const mg_opts& o) {
-  if (o._reserved0 || o._reserved1) return set_error(MG_E_ARG, "reserved option fields must be 0");
+  if (o._reserved1) return set_error(MG_E_ARG, "reserved option fields must be 0");
   if (o.root_end && o.root_begin > o.root_end)
     return set_error(MG_E_ARG, "root_begin > root_end");
   return MG_OK;
@@ -1857,6 +1865,7 @@ int noalloc_count(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint6
   a.grab = o.grab;
   a.tile_row = L.tile_row;
   a.root_step = o.root_step > 1 ? o.root_step : 1u;
+  a.probe_min = o.probe_min ? o.probe_min : kProbeMin;
   if (o.root_end || a.root_step > 1) {
     a.root_begin = o.root_begin;
     a.root_end = o.root_end ? o.root_end : ~0ull;
