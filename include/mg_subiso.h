@@ -104,7 +104,7 @@ typedef struct mg_opts {
   uint32_t probe_min;        /* a probe into the label slice of a hub uses the
                                 hub's bitmap when the slice has at least this
                                 many entries, binary search otherwise
-                                (0 = 32, 1 = always the bitmap)              */
+                                (0 or 1: always the bitmap)                  */
   uint32_t _reserved1;       /* must be 0                                    */
   uint64_t mem_budget_bytes; /* cap on enumeration scratch; 0 = auto        */
   uint64_t root_begin;       /* level-0 candidates [root_begin, root_end) of  */

@@ -107,7 +107,7 @@ static int ws_alloc(Workspace* ws, void** p, size_t bytes) {
 }
 
 constexpr uint64_t kDefaultCap = 1ull << 24;
-constexpr uint32_t kProbeMin = 32;  // default shortest hub slice probed by bitmap
+constexpr uint32_t kProbeMin = 1;  // default: every hub slice is probed in the bitmap
 constexpr int SCAN_TILE = 4096;
 constexpr int EXPAND_BLOCK = 256;                 // elements per expand tile
 constexpr uint64_t kSegment = 1ull << 26;         // elements per expand launch
