@@ -84,6 +84,8 @@ def parse():
     p.add_argument("--no-gar", action="store_true", help="skip the GAR match timing")
     p.add_argument("--no-batch", action="store_true",
                    help="skip the batched-workload measurement")
+    p.add_argument("--hub-bytes", type=int, default=None,
+                   help="hub-bitmap budget of the upload (profiling runs; default: library)")
     return p.parse_args()
 
 
@@ -102,6 +104,13 @@ def config(scale, n, m, only=""):
             "queries": names, "order": "reference", "mode": "count",
             "l2": "inputs larger than L2 (graph + indices > 1 GB) and a 256 MiB L2 flush "
                   "before every step"}
+
+
+# DRAM bytes (read + write) per expand-kernel launch of this workload, from
+# the one-pass ncu launch list summarised in
+# profiles/launches_rmat22_5queries_traffic.md (mean over the expand launches
+# of one step).
+EXPAND_TRAFFIC_BYTES = 230_592_092
 
 
 def peaks():
@@ -400,7 +409,7 @@ def run_mine(args):
     torch.cuda.set_device(device)
     # Level-0 candidates of this rank: positions rank, rank + world, ...
     shard = mg.shard_strided(rank, world)
-    dg = mg.DeviceGraph(g, device)
+    dg = mg.DeviceGraph(g, device, hub_bytes=args.hub_bytes)
     info = dg.info
     _log("graph uploaded")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device=f"cuda:{device}")
@@ -471,18 +480,38 @@ def run_mine(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
 
+    # Kernel-timing pass (after the timed region): every expand launch between
+    # a CUDA event pair on the library's stream.
+    expand_ms, expand_launches = 0.0, 0
+    for q in qs:
+        _, st = dg.count(q, stats=True, kernel_events=1, **shard)
+        expand_ms += st["expand_ms"]
+        expand_launches += st["expand_launches"]
+    _log("kernel-timing pass done")
+
     same = None
     if cpu_rows is not None:
         same = same_work(dg, qs, names, cpu_rows, device, g)
         _log(f"same-work check: equal={same['equal']}")
 
     peak, peak_kind = peaks()
-    achieved = balgc / (ms_step / 1e3) / 1e9
+    # The dominant kernel is the expand kernel (over 90% of device time): its
+    # algorithmic bytes per launch are the step's B_alg (count-mode
+    # definition) over its launches, its duration the event-timed mean.
+    per_launch_bytes = balgc / max(1, expand_launches)
+    per_launch_s = expand_ms / 1e3 / max(1, expand_launches)
+    achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None,
-                "basis": f"B_alg (count-mode definition) per step / device time per step; "
-                         f"peak {peak_kind} copy bandwidth",
-                "balg_count_bytes_per_step": balgc, "balg_bytes_per_step": balg}
+                "frac": achieved / peak, "traffic": EXPAND_TRAFFIC_BYTES,
+                "kernel": "k_expand (all launch shapes)",
+                "basis": "B_alg (count-mode definition, the merge-intersection byte count) "
+                         "per expand launch / CUDA-event mean launch duration; peak "
+                         f"{peak_kind} copy bandwidth; traffic = ncu DRAM read+write bytes "
+                         "per expand launch of this workload",
+                "expand_launches_per_step": expand_launches,
+                "expand_ms_per_step": expand_ms,
+                "balg_count_bytes_per_step": balgc, "balg_bytes_per_step": balg,
+                "step_rate_gbs": balgc / (ms_step / 1e3) / 1e9}
     batch = None
     if world == 1 and not args.no_batch and args.scale == 22 and not args.queries:
         batch = batched_workload(g, dg)

@@ -105,7 +105,10 @@ typedef struct mg_opts {
                                 hub's bitmap when the slice has at least this
                                 many entries, binary search otherwise
                                 (0 or 1: always the bitmap)                  */
-  uint32_t _reserved1;       /* must be 0                                    */
+  uint32_t kernel_events;    /* 1: time every expand-kernel launch with a CUDA
+                                event pair (mg_stats.expand_ms); each launch
+                                then waits for the previous one on the host,
+                                so use it for measurement passes only        */
   uint64_t mem_budget_bytes; /* cap on enumeration scratch; 0 = auto        */
   uint64_t root_begin;       /* level-0 candidates [root_begin, root_end) of  */
   uint64_t root_end;         /* the first position's label bucket; 0,0 = all  */
@@ -131,6 +134,9 @@ typedef struct mg_stats {
   uint64_t launches;         /* kernels launched by this call                */
   uint64_t chunks;           /* level chunks processed                       */
   uint64_t elements;         /* candidate elements expanded                  */
+  double   expand_ms;        /* summed durations of the expand-kernel launches
+                                (opts->kernel_events = 1, else 0)            */
+  uint64_t expand_launches;  /* expand-kernel launches                       */
 } mg_stats;
 
 typedef struct mg_graph_info {

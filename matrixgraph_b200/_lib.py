@@ -59,7 +59,7 @@ class Opts(C.Structure):
     _fields_ = [("order", C.c_int32), ("filters", C.c_uint32), ("given_order", P32),
                 ("model", C.c_void_p), ("chunk_rows", C.c_uint64), ("grab", C.c_uint32),
                 ("root_step", C.c_uint32), ("probe_min", C.c_uint32),
-                ("_reserved1", C.c_uint32), ("mem_budget_bytes", C.c_uint64),
+                ("kernel_events", C.c_uint32), ("mem_budget_bytes", C.c_uint64),
                 ("root_begin", C.c_uint64), ("root_end", C.c_uint64),
                 ("no_tail", C.c_uint32), ("_reserved", C.c_uint32),
                 ("max_elements", C.c_uint64)]
@@ -70,7 +70,8 @@ class Stats(C.Structure):
                 ("level_rows", C.c_uint64 * (MG_MAX_QUERY_VERTICES + 1)),
                 ("balg_bytes", C.c_uint64), ("balg_count_bytes", C.c_uint64),
                 ("device_ms", C.c_double), ("launches", C.c_uint64), ("chunks", C.c_uint64),
-                ("elements", C.c_uint64)]
+                ("elements", C.c_uint64), ("expand_ms", C.c_double),
+                ("expand_launches", C.c_uint64)]
 
 
 class GraphInfo(C.Structure):

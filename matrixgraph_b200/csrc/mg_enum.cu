@@ -72,7 +72,7 @@ struct Workspace {
   uint32_t counts_cap = 0;
   PlanDev* plans = nullptr;
   uint32_t plans_cap = 0;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
   std::vector<void*> allocs;
   uint64_t bytes = 0;
 };
@@ -89,6 +89,8 @@ void free_workspace(Workspace* ws) {
   if (ws->h_ctr) cudaFreeHost(ws->h_ctr);
   if (ws->ev0) cudaEventDestroy(ws->ev0);
   if (ws->ev1) cudaEventDestroy(ws->ev1);
+  if (ws->ev2) cudaEventDestroy(ws->ev2);
+  if (ws->ev3) cudaEventDestroy(ws->ev3);
   delete ws;
 }
 
@@ -131,6 +133,8 @@ static int ensure_ws(DevGraph* dg, uint64_t cap, int levels, uint32_t nq) {
     MG_CK(cudaMallocHost((void**)&ws->h_ctr, C_NUM * 8));
     MG_CK(cudaEventCreate(&ws->ev0));
     MG_CK(cudaEventCreate(&ws->ev1));
+    MG_CK(cudaEventCreate(&ws->ev2));
+    MG_CK(cudaEventCreate(&ws->ev3));
     ws->bsum_cap = uint32_t((std::max<uint64_t>(cap, ws->rows0) + SCAN_TILE - 1) / SCAN_TILE + 1);
     if ((rc = ws_alloc(ws, (void**)&ws->bsum, uint64_t(ws->bsum_cap) * 8))) return rc;
     if ((rc = ws_alloc(ws, (void**)&ws->tile_row, (kSegment / EXPAND_BLOCK + 2) * 4))) return rc;
@@ -742,7 +746,13 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
   // hub row's elements still spread over many blocks.
   __shared__ unsigned long long s_base, s_wbase;
   __shared__ uint32_t s_wcnt[EXPAND_BLOCK / 32];
-  const uint64_t grab = a.grab ? a.grab : 4;
+  // Tiles per grab: about 16 grabs per block over the launch (fewer queue
+  // atomics and barriers), at least 4, at most 32.
+  uint64_t grab = a.grab;
+  if (!grab) {
+    grab = ntiles / (uint64_t(gridDim.x) * 16);
+    grab = grab < 4 ? 4 : (grab > 32 ? 32 : grab);
+  }
   for (;;) {
     if (threadIdx.x == 0) s_base = atomicAdd(&a.ctr[C_TILE], (unsigned long long)grab);
     __syncthreads();
@@ -904,8 +914,9 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
       }  // X_EMIT
       if constexpr ((MODE & X_WRITE) != 0) __syncthreads();  // s_wcnt / s_wbase reused next tile
     }
-    // Once per grab: fold the per-thread counts of a warp that holds one query.
-    acc_flush_warp(a, cnt_q, i, cnt, s1, sk, s2, false);
+    // Once per grab in a batch: fold the per-thread counts of a warp that holds
+    // one query (a single query's counts are folded once, at the end).
+    if (a.in.qid) acc_flush_warp(a, cnt_q, i, cnt, s1, sk, s2, false);
   }  // grab loop
   acc_flush_warp(a, cnt_q, i, cnt, s1, sk, s2, true);
   bal = warp_sum(bal);
@@ -1041,7 +1052,8 @@ struct EmitBuf {
 };
 
 struct RunResult {
-  uint64_t balg = 0, balgc = 0, launches = 0, chunks = 0, elements = 0;
+  uint64_t balg = 0, balgc = 0, launches = 0, chunks = 0, elements = 0, expand_launches = 0;
+  double expand_ms = 0;
   uint64_t surv[MAXK + 2] = {};
   uint64_t emitted = 0;
   double ms = 0;
@@ -1331,8 +1343,17 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
         k_tile_rows<<<grid_for(uint64_t(ntiles) + 1, 256, sms * 16), 256, 0, st>>>(
             ws->woff[lvl], R[lvl], s0, s1, ntiles, ws->tile_row);
         MG_CK(cudaMemsetAsync(ws->ctr + C_TILE, 0, 8, st));
+        if (o.kernel_events) MG_CK(cudaEventRecord(ws->ev2, st));
         launch_expand(a, plans.data(), nq, count_mode, writes[lvl],
                       grid_for(s1 - s0, EXPAND_BLOCK, sms * 8), st);
+        if (o.kernel_events) {
+          MG_CK(cudaEventRecord(ws->ev3, st));
+          MG_CK(cudaEventSynchronize(ws->ev3));
+          float kms = 0;
+          MG_CK(cudaEventElapsedTime(&kms, ws->ev2, ws->ev3));
+          res->expand_ms += kms;
+        }
+        res->expand_launches++;
         res->launches += 2;
       }
       res->chunks++;
@@ -1465,7 +1486,6 @@ static mg_opts resolve_opts(const mg_opts* o) {
 
 // Checks that do not depend on the query or the graph.
 static int check_opts(const mg_opts& o) {
-  if (o._reserved1) return set_error(MG_E_ARG, "reserved option fields must be 0");
   if (o.root_end && o.root_begin > o.root_end)
     return set_error(MG_E_ARG, "root_begin > root_end");
   return MG_OK;
@@ -1484,6 +1504,8 @@ static void fill_stats(mg_stats* st, const PlanDev& P, const RunResult& res, uin
   st->launches = res.launches;
   st->chunks = res.chunks;
   st->elements = res.elements;
+  st->expand_ms = res.expand_ms;
+  st->expand_launches = res.expand_launches;
 }
 
 static int prepare(DevGraph* dg, const mg_csr_view* q, const mg_opts& o, PlanDev* P) {
@@ -1595,6 +1617,8 @@ int subiso_batch(DevGraph* dg, const mg_csr_view* const* qs, uint32_t nq, const 
     st->launches = res.launches;
     st->chunks = res.chunks;
     st->elements = res.elements;
+    st->expand_ms = res.expand_ms;
+    st->expand_launches = res.expand_launches;
   }
   return MG_OK;
 }

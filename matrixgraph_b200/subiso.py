@@ -33,7 +33,7 @@ ORDERS = {"reference": L.MG_ORDER_REFERENCE, "heuristic": L.MG_ORDER_REFERENCE,
 
 def make_opts(order="reference", filters=L.MG_FILTER_ALL, chunk_rows=0, given_order=None,
               model=None, root_range=None, mem_budget_bytes=0, root_step=0,
-              grab=0, no_tail=0, max_elements=0, probe_min=0):
+              grab=0, no_tail=0, max_elements=0, probe_min=0, kernel_events=0):
     o = L.default_opts()
     o.no_tail = no_tail
     o.max_elements = max_elements
@@ -43,6 +43,7 @@ def make_opts(order="reference", filters=L.MG_FILTER_ALL, chunk_rows=0, given_or
     o.mem_budget_bytes = mem_budget_bytes
     o.root_step = root_step
     o.probe_min = probe_min
+    o.kernel_events = kernel_events
     o.grab = grab
     keep = None
     if given_order is not None:
@@ -61,7 +62,8 @@ def stats_dict(st: L.Stats) -> dict:
     return {"k": k, "order": list(st.order[:k]), "level_rows": list(st.level_rows[:k + 1]),
             "balg_bytes": st.balg_bytes, "balg_count_bytes": st.balg_count_bytes,
             "device_ms": st.device_ms, "launches": st.launches, "chunks": st.chunks,
-            "elements": st.elements}
+            "elements": st.elements, "expand_ms": st.expand_ms,
+            "expand_launches": st.expand_launches}
 
 
 def plan_order(q: CSRGraph, order="reference", graph: "DeviceGraph | None" = None,
