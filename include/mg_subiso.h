@@ -115,12 +115,18 @@ typedef struct mg_opts {
   uint32_t no_tail;          /* closed-form count of a two-position pendant
                                 tail (count mode): 0 or 2 = whenever the plan
                                 ends in one, 1 = never                       */
-  uint32_t _reserved;
+  uint32_t lanes;            /* batch counts: queries run as fixed launch
+                                sequences on this many concurrent streams,
+                                every size read on the device, one host sync
+                                per batch (0 = 8); MG_LANES_SHARED = one
+                                level-synchronous run over shared tables     */
   uint64_t max_elements;     /* work budget in candidate elements (0 = none):
                                 a single-query call above it returns
                                 MG_E_LIMIT; in a batch it applies per query
                                 and a query above it reports UINT64_MAX      */
 } mg_opts;
+
+#define MG_LANES_SHARED 0xFFFFFFFFu
 
 /* Per-call statistics (optional out-parameter of the *_ex entry points). */
 typedef struct mg_stats {

@@ -29,6 +29,8 @@ MG_ORDER_STRONG = 1
 MG_ORDER_LEARNED = 2
 MG_ORDER_GIVEN = 3
 
+MG_LANES_SHARED = 0xFFFFFFFF
+
 MG_FILTER_DEGREE = 1
 MG_FILTER_NLB = 2
 MG_FILTER_ALL = 3
@@ -61,7 +63,7 @@ class Opts(C.Structure):
                 ("root_step", C.c_uint32), ("probe_min", C.c_uint32),
                 ("kernel_events", C.c_uint32), ("mem_budget_bytes", C.c_uint64),
                 ("root_begin", C.c_uint64), ("root_end", C.c_uint64),
-                ("no_tail", C.c_uint32), ("_reserved", C.c_uint32),
+                ("no_tail", C.c_uint32), ("lanes", C.c_uint32),
                 ("max_elements", C.c_uint64)]
 
 

@@ -91,6 +91,7 @@ struct TailKey {
 };
 
 struct Workspace;  // enumeration scratch (mg_enum.cu)
+struct LaneSet;    // batch lane pipelines (mg_enum.cu)
 
 // Host object behind the opaque dgraph handle.
 struct DevGraph {
@@ -104,6 +105,7 @@ struct DevGraph {
   std::vector<uint32_t> h_bucket_off;
   std::vector<void*> allocs;
   Workspace* ws = nullptr;
+  LaneSet* lanes = nullptr;
   std::mutex mu;
   ~DevGraph();
 };

@@ -79,8 +79,13 @@ struct Workspace {
 
 // Counter slots.
 enum : int {
-  C_OUT = 0, C_BALG = 1, C_BALGC = 2, C_ERR = 3, C_EMIT = 4, C_HNEW = 5, C_TILE = 6, C_SURV = 8,
-  C_NUM = 8 + MAXK + 2
+  C_OUT = 0, C_BALG = 1, C_BALGC = 2, C_ERR = 3, C_EMIT = 4, C_HNEW = 5, C_TILE = 6,
+  // Lane pipeline (sizes live on the device), one slot per level l:
+  C_LOUT = 8,                // rows the expand of level l wrote (= rows of level l+1)
+  C_LTILE = C_LOUT + MAXK,   // work-queue position of the expand of level l
+  C_LT = C_LTILE + MAXK,     // candidate elements of level l
+  C_LSCAN = C_LT + MAXK,     // tile counter of the work/scan kernel of level l
+  C_NUM = C_LSCAN + MAXK
 };
 
 void free_workspace(Workspace* ws) {
@@ -212,7 +217,23 @@ struct StepArgs {
   uint32_t tail_dense;
   const unsigned long long* tdA;
   const unsigned long long* tdAD;
+  // Lane pipeline: row and element counts come from the counters (C_LOUT,
+  // C_LT), the expand's queue and output use the per-level slots, and no
+  // host value of R, t0 or t1 is read.
+  uint32_t lane;
+  uint32_t out_slot, tile_slot;  // counter slots of the output rows / work queue
+  uint64_t cap_rows;             // rows of a lane's level table
+  uint64_t seg_cap;              // elements one lane expand launch can tile
+  unsigned long long* scan_status;  // look-back words of the work/scan kernel
+  uint32_t spin_limit;           // bounded device waits (iterations)
 };
+
+// Rows of the input table of a lane launch at level a.level.
+__device__ __forceinline__ uint64_t lane_rows(const StepArgs& a) {
+  if (a.level == 0) return 1;
+  const uint64_t r = a.ctr[C_LOUT + a.level - 1];
+  return r < a.cap_rows ? r : a.cap_rows;
+}
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t l = threadIdx.x & 31;
@@ -518,6 +539,58 @@ __device__ __forceinline__ void tail_count(const StepArgs& a, const PlanDev& P, 
 // Work kernel: per row, the driving slice (shortest backward slice, or the
 // label bucket for a position without backward neighbours) and the
 // algorithmic-byte charge of extending the row.
+// Driving slice of table row r at position a.level: its length (the row's
+// candidate elements, 0 when nothing is to be expanded), start and constraint
+// index (DCI_BUCKET: the label bucket), and the row's algorithmic-byte
+// charges (full-slice and count-mode definitions).
+__device__ __forceinline__ uint32_t row_work(const StepArgs& a, const PlanDev& P, uint64_t r,
+                                             uint32_t q, uint32_t& bs, uint8_t& bci,
+                                             unsigned long long& ch, unsigned long long& chc) {
+  const GraphDev& g = a.g;
+  const uint32_t i = a.level;
+  const uint32_t lab = P.label[i];
+  const uint32_t nc = P.ncons[i];
+  uint32_t best;
+  bs = 0;
+  bci = DCI_BUCKET;
+  ch = chc = 0;
+  if (P.zero) {
+    best = 0;
+  } else if (nc == 0) {
+    bs = __ldg(g.bucket_off + lab);
+    best = __ldg(g.bucket_off + lab + 1) - bs;
+    if (i == 0 && a.root_end) {
+      const uint64_t rb = a.root_begin < best ? a.root_begin : uint64_t(best);
+      const uint64_t re = a.root_end < best ? a.root_end : uint64_t(best);
+      bs += uint32_t(rb);
+      best = re > rb ? uint32_t((re - rb + a.root_step - 1) / a.root_step) : 0u;
+    }
+    ch = chc = (unsigned long long)best * (12ull + 4ull * g.W);
+  } else {
+    best = FULL;
+    for (uint32_t c = 0; c < nc; ++c) {
+      const uint32_t cs = P.cons[i][c];
+      const uint32_t y = a.in.col[cs & 0xFF][r];
+      uint32_t s, e;
+      slice_of(g, cs >> 8, y, lab, s, e);
+      ch += 8ull + 4ull * (e - s);
+      if (e - s < best) {
+        best = e - s;
+        bs = s;
+        bci = uint8_t(c);
+      }
+    }
+    chc = (i + 1 == P.k && P.last_o1) ? 8ull : ch;
+  }
+  if (a.q_budget && best) {
+    // Per-query budget: a query whose scheduled elements pass the budget
+    // stops expanding (its count is reported as unknown).
+    const unsigned long long before = atomicAdd(&a.q_elems[q], (unsigned long long)best);
+    if (before + best > a.q_budget) best = 0;
+  }
+  return best;
+}
+
 __global__ void __launch_bounds__(256) k_work(StepArgs a) {
   unsigned long long bal = 0, balc = 0, tcnt = 0, tpre = 0;
   uint32_t tq = 0;
@@ -532,7 +605,6 @@ __global__ void __launch_bounds__(256) k_work(StepArgs a) {
     const uint32_t q = a.in.qid ? a.in.qid[r] : 0u;
     const PlanDev& P = a.plans[q];
     const uint32_t lab = P.label[i];
-    const uint32_t nc = P.ncons[i];
     uint32_t best, bs = 0;
     uint8_t bci = DCI_BUCKET;
     unsigned long long ch = 0, chc = 0;
@@ -560,40 +632,7 @@ __global__ void __launch_bounds__(256) k_work(StepArgs a) {
       balc += chc;
       continue;
     }
-    if (P.zero) {
-      best = 0;
-    } else if (nc == 0) {
-      bs = __ldg(g.bucket_off + lab);
-      best = __ldg(g.bucket_off + lab + 1) - bs;
-      if (i == 0 && a.root_end) {
-        const uint64_t rb = a.root_begin < best ? a.root_begin : uint64_t(best);
-        const uint64_t re = a.root_end < best ? a.root_end : uint64_t(best);
-        bs += uint32_t(rb);
-        best = re > rb ? uint32_t((re - rb + a.root_step - 1) / a.root_step) : 0u;
-      }
-      ch = chc = (unsigned long long)best * (12ull + 4ull * g.W);
-    } else {
-      best = FULL;
-      for (uint32_t c = 0; c < nc; ++c) {
-        const uint32_t cs = P.cons[i][c];
-        const uint32_t y = a.in.col[cs & 0xFF][r];
-        uint32_t s, e;
-        slice_of(g, cs >> 8, y, lab, s, e);
-        ch += 8ull + 4ull * (e - s);
-        if (e - s < best) {
-          best = e - s;
-          bs = s;
-          bci = uint8_t(c);
-        }
-      }
-      chc = (i + 1 == P.k && P.last_o1) ? 8ull : ch;
-    }
-    if (a.q_budget && best) {
-      // Per-query budget: a query whose scheduled elements pass the budget
-      // stops expanding (its count is reported as unknown).
-      const unsigned long long before = atomicAdd(&a.q_elems[q], (unsigned long long)best);
-      if (before + best > a.q_budget) best = 0;
-    }
+    best = row_work(a, P, r, q, bs, bci, ch, chc);
     a.work[r] = best;
     a.dstart[r] = bs;
     a.dci[r] = bci;
@@ -737,7 +776,13 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
   const uint32_t i = a.level;
   const GraphDev& g = a.g;
   const uint32_t lane = threadIdx.x & 31;
-  const uint64_t span = a.t1 - a.t0;
+  uint64_t t0 = a.t0, t1 = a.t1;
+  if (a.lane) {  // lane pipeline: this level's elements, capped (k_tile_rows_lane flags it)
+    t0 = 0;
+    t1 = a.ctr[C_LT + i];
+    if (t1 > a.seg_cap) t1 = a.seg_cap;
+  }
+  const uint64_t span = t1 - t0;
   const uint64_t ntiles = (span + EXPAND_BLOCK - 1) / EXPAND_BLOCK;
   unsigned long long cnt = 0, bal = 0, balc = 0, s1 = 0, sk = 0, s2 = 0;
   uint32_t cnt_q = 0;
@@ -754,15 +799,15 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
     grab = grab < 4 ? 4 : (grab > 32 ? 32 : grab);
   }
   for (;;) {
-    if (threadIdx.x == 0) s_base = atomicAdd(&a.ctr[C_TILE], (unsigned long long)grab);
+    if (threadIdx.x == 0) s_base = atomicAdd(&a.ctr[a.tile_slot], (unsigned long long)grab);
     __syncthreads();
     const uint64_t gbase = s_base;
     __syncthreads();
     if (gbase >= ntiles) break;
     const uint64_t gend = min(gbase + grab, ntiles);
     for (uint64_t tile = gbase; tile < gend; ++tile) {
-      const uint64_t tb = a.t0 + tile * EXPAND_BLOCK;
-      const uint64_t te = min(tb + EXPAND_BLOCK, a.t1);
+      const uint64_t tb = t0 + tile * EXPAND_BLOCK;
+      const uint64_t te = min(tb + EXPAND_BLOCK, t1);
       const uint32_t rlo = __ldg(a.tile_row + tile), rhi = __ldg(a.tile_row + tile + 1);
       const uint64_t t = tb + threadIdx.x;
       const bool valid = t < te;
@@ -872,7 +917,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
             s_wcnt[w] = tot;
             tot += c;
           }
-          s_wbase = tot ? atomicAdd(&a.ctr[C_OUT], (unsigned long long)tot) : 0ull;
+          s_wbase = tot ? atomicAdd(&a.ctr[a.out_slot], (unsigned long long)tot) : 0ull;
         }
         __syncthreads();
         if (wm) {
@@ -925,6 +970,151 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
     atomicAdd(&a.ctr[C_BALG], bal);
     atomicAdd(&a.ctr[C_BALGC], balc);
   }
+}
+
+// ---- lane pipeline kernels --------------------------------------------------
+// Look-back words of the single-pass work/scan: [epoch:20 | status:2 | value:42].
+constexpr int LB_VALUE_BITS = 42;
+constexpr unsigned long long LB_AGG = 1, LB_INC = 2;
+constexpr int WS_ROWS = 1024;  // rows per work/scan tile (4 per thread)
+
+__device__ __forceinline__ unsigned long long lb_word(uint32_t epoch, unsigned long long st,
+                                                      unsigned long long v) {
+  return (uint64_t(epoch) << (LB_VALUE_BITS + 2)) | (st << LB_VALUE_BITS) |
+         (v & ((1ull << LB_VALUE_BITS) - 1));
+}
+
+// Work + scan of one lane level in one pass: tiles of WS_ROWS rows are taken
+// in launch order from a counter; each computes its rows' driving slices,
+// publishes its sum, and adds the sums of the tiles before it (decoupled
+// look-back: a predecessor's inclusive prefix, or its sum and keep looking).
+// A tile only ever waits for tiles claimed before it, whose blocks are
+// running, and every wait gives up after spin_limit polls (ERR_TIMEOUT).
+// The last tile writes the level's element total to woff[R] and C_LT.
+__global__ void __launch_bounds__(256) k_work_scan(StepArgs a, uint32_t epoch) {
+  const uint32_t i = a.level;
+  const uint64_t R = lane_rows(a);
+  const uint64_t ntiles = (R + WS_ROWS - 1) / WS_ROWS;
+  unsigned long long bal = 0, balc = 0;
+  __shared__ uint32_t s_tile;
+  __shared__ unsigned long long s_prefix;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = uint32_t(atomicAdd(&a.ctr[C_LSCAN + i], 1ull));
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    __syncthreads();
+    if (tile >= ntiles) break;
+    const uint64_t base = tile * WS_ROWS + uint64_t(threadIdx.x) * 4;
+    unsigned long long v[4], sum = 0;
+    for (int j = 0; j < 4; ++j) {
+      const uint64_t r = base + j;
+      v[j] = 0;
+      if (r < R) {
+        const PlanDev& P = a.plans[0];
+        uint32_t bs;
+        uint8_t bci;
+        unsigned long long ch, chc;
+        const uint32_t w = row_work(a, P, r, 0, bs, bci, ch, chc);
+        a.work[r] = w;
+        a.dstart[r] = bs;
+        a.dci[r] = bci;
+        bal += ch;
+        balc += chc;
+        v[j] = w;
+        sum += w;
+      }
+    }
+    unsigned long long tot;
+    const unsigned long long ex = block_exclusive_scan(sum, &tot);
+    if (threadIdx.x == 0) {
+      unsigned long long* st = a.scan_status;
+      atomicExch(st + tile, lb_word(epoch, tile == 0 ? LB_INC : LB_AGG, tot));
+      unsigned long long prefix = 0;
+      for (int64_t t = int64_t(tile) - 1; t >= 0; --t) {
+        unsigned long long w = 0;
+        uint32_t spins = 0;
+        for (;;) {
+          w = atomicAdd(st + t, 0ull);
+          if ((w >> (LB_VALUE_BITS + 2)) == epoch && ((w >> LB_VALUE_BITS) & 3ull)) break;
+          if (++spins > a.spin_limit) {
+            atomicOr(&a.ctr[C_ERR], (unsigned long long)ERR_TIMEOUT);
+            w = lb_word(epoch, LB_INC, 0);
+            break;
+          }
+          __nanosleep(64);
+        }
+        prefix += w & ((1ull << LB_VALUE_BITS) - 1);
+        if (((w >> LB_VALUE_BITS) & 3ull) == LB_INC) break;
+      }
+      if (tile > 0) atomicExch(st + tile, lb_word(epoch, LB_INC, prefix + tot));
+      if (prefix + tot >= (1ull << LB_VALUE_BITS))
+        atomicOr(&a.ctr[C_ERR], (unsigned long long)ERR_OVERFLOW);
+      s_prefix = prefix;
+      if (tile + 1 == ntiles) {
+        a.woff[R] = prefix + tot;
+        a.ctr[C_LT + i] = prefix + tot;
+      }
+    }
+    __syncthreads();
+    unsigned long long o = s_prefix + ex;
+    for (int j = 0; j < 4; ++j) {
+      const uint64_t r = base + j;
+      if (r < R) a.woff[r] = o;
+      o += v[j];
+    }
+  }
+  bal = warp_sum(bal);
+  balc = warp_sum(balc);
+  if ((threadIdx.x & 31) == 0 && (bal | balc)) {
+    atomicAdd(&a.ctr[C_BALG], bal);
+    atomicAdd(&a.ctr[C_BALGC], balc);
+  }
+}
+
+// First row of every expand tile of a lane level (the element total is read
+// from the device; a total beyond the lane's tile buffer is flagged and the
+// query is re-run on the chunked path).
+__global__ void __launch_bounds__(256) k_tile_rows_lane(StepArgs a) {
+  const uint64_t R = lane_rows(a);
+  uint64_t T = a.ctr[C_LT + a.level];
+  if (T > a.seg_cap) {
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+      atomicOr(&a.ctr[C_ERR], (unsigned long long)ERR_OVERFLOW);
+    T = a.seg_cap;
+  }
+  if (T == 0 || R == 0) return;
+  const uint64_t ntiles = (T + EXPAND_BLOCK - 1) / EXPAND_BLOCK;
+  for (uint64_t j = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; j <= ntiles;
+       j += uint64_t(gridDim.x) * blockDim.x) {
+    uint64_t t = j * EXPAND_BLOCK;
+    if (t > T - 1) t = T - 1;
+    const_cast<uint32_t*>(a.tile_row)[j] = find_row(a.woff, 0, uint32_t(R - 1), t);
+  }
+}
+
+// End of one query on a lane: its count, survivors per prefix length and
+// error bits go to the batch arrays (entry q), and the lane's per-query state
+// is cleared for the next query.  A query past its element budget reports
+// UINT64_MAX.
+__global__ void k_lane_done(unsigned long long* ctr, unsigned long long* counts,
+                            unsigned long long* lvl, unsigned long long* qel,
+                            unsigned long long budget, uint32_t q,
+                            unsigned long long* out_counts, unsigned long long* out_lvl,
+                            unsigned long long* out_err) {
+  const uint32_t t = threadIdx.x;
+  if (t <= MAXK) {
+    out_lvl[uint64_t(q) * (MAXK + 1) + t] = lvl[t];
+    lvl[t] = 0;
+  }
+  __syncwarp();
+  if (t == 0) {
+    out_counts[q] = (budget && qel[0] > budget) ? ~0ull : counts[0];
+    out_err[q] = ctr[C_ERR];
+    counts[0] = 0;
+    qel[0] = 0;
+    ctr[C_ERR] = 0;
+  }
+  for (int c = C_LOUT + int(t); c < C_NUM; c += 32) ctr[c] = 0;
 }
 
 __global__ void k_iota(uint32_t* p, uint32_t n) {
@@ -1053,6 +1243,7 @@ struct EmitBuf {
 
 struct RunResult {
   uint64_t balg = 0, balgc = 0, launches = 0, chunks = 0, elements = 0, expand_launches = 0;
+  uint64_t reruns = 0;  // batch queries counted again on the chunked path
   double expand_ms = 0;
   uint64_t surv[MAXK + 2] = {};
   uint64_t emitted = 0;
@@ -1145,6 +1336,8 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
   }
   a.root_step = o.root_step > 1 ? o.root_step : 1u;
   a.probe_min = o.probe_min ? o.probe_min : kProbeMin;
+  a.out_slot = C_OUT;
+  a.tile_slot = C_TILE;
   if (o.root_end || a.root_step > 1) {
     a.root_begin = o.root_begin;
     a.root_end = o.root_end ? o.root_end : ~0ull;
@@ -1573,6 +1766,319 @@ int subiso_emit(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint32_
   return MG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Batch lane pipeline
+//
+// Each query of a batch runs as a fixed sequence of launches (per level: the
+// single-pass work/scan, the tile-row lookup, the expand) whose kernels read
+// every size from device counters, so nothing returns to the host between
+// levels or between queries.  Queries are dealt round-robin to `lanes`
+// streams that run concurrently; each lane owns level tables of `cap` rows.
+// The host waits once per batch; a query whose rows or elements did not fit
+// its lane (ERR_OVERFLOW) is counted again on the chunked path, which has no
+// size limit.
+// ---------------------------------------------------------------------------
+struct Lane {
+  cudaStream_t st = nullptr;
+  unsigned long long *ctr = nullptr, *counts = nullptr, *lvl = nullptr, *qel = nullptr;
+  unsigned long long* status = nullptr;  // look-back words of the work/scan kernel
+  uint32_t* tile_row = nullptr;
+  uint32_t* col[MAXK][MAXK] = {};
+  uint32_t* work[MAXK] = {};
+  uint64_t* woff[MAXK] = {};
+  uint32_t* dstart[MAXK] = {};
+  uint8_t* dci[MAXK] = {};
+  uint32_t epoch = 0;
+};
+
+struct LaneSet {
+  uint64_t cap = 0, seg_cap = 0;
+  uint32_t kmax = 0;
+  std::vector<Lane> lanes;
+  std::vector<void*> allocs;
+  unsigned long long *r_counts = nullptr, *r_lvl = nullptr, *r_err = nullptr;
+  uint32_t r_cap = 0;
+  PlanDev* plans = nullptr;
+  uint32_t plans_cap = 0;
+  unsigned long long *tdA = nullptr, *tdAD = nullptr;
+  uint64_t td_cap = 0;
+  TailKey* tkeys = nullptr;
+  uint32_t tkeys_cap = 0;
+  cudaEvent_t ev_start = nullptr, ev_end = nullptr;
+};
+
+constexpr uint64_t kLaneCap = 1ull << 20;     // rows per lane level table
+constexpr uint64_t kLaneSegment = 1ull << 26; // elements per lane expand launch
+constexpr uint32_t kLanes = 8;
+constexpr uint32_t kSpinLimit = 1u << 22;     // polls of a look-back wait (~0.3 s)
+constexpr uint32_t kEpochMax = (1u << 20) - 1;
+
+void free_lanes(LaneSet* ls) {
+  if (!ls) return;
+  for (Lane& l : ls->lanes)
+    if (l.st) cudaStreamDestroy(l.st);
+  for (void* p : ls->allocs) cudaFree(p);
+  if (ls->ev_start) cudaEventDestroy(ls->ev_start);
+  if (ls->ev_end) cudaEventDestroy(ls->ev_end);
+  delete ls;
+}
+
+static int lane_alloc(LaneSet* ls, void** p, size_t bytes) {
+  *p = nullptr;
+  cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return set_error(MG_E_OOM, "lane scratch: cudaMalloc(%zu) failed: %s", bytes,
+                     cudaGetErrorString(e));
+  }
+  ls->allocs.push_back(*p);
+  return MG_OK;
+}
+
+static int ensure_lanes(DevGraph* dg, uint32_t nl, uint64_t cap, uint32_t kmax) {
+  LaneSet*& ls = dg->lanes;
+  if (ls && (ls->lanes.size() != nl || ls->cap != cap || ls->kmax < kmax)) {
+    cudaDeviceSynchronize();
+    free_lanes(ls);
+    ls = nullptr;
+  }
+  if (ls) return MG_OK;
+  ls = new LaneSet();
+  ls->cap = cap;
+  ls->seg_cap = kLaneSegment;
+  ls->kmax = std::max<uint32_t>(kmax, 8);
+  MG_CK(cudaEventCreateWithFlags(&ls->ev_start, cudaEventDisableTiming));
+  MG_CK(cudaEventCreateWithFlags(&ls->ev_end, cudaEventDisableTiming));
+  ls->lanes.resize(nl);
+  int rc;
+  for (Lane& L : ls->lanes) {
+    MG_CK(cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking));
+    if ((rc = lane_alloc(ls, (void**)&L.ctr, C_NUM * 8))) return rc;
+    if ((rc = lane_alloc(ls, (void**)&L.counts, 8))) return rc;
+    if ((rc = lane_alloc(ls, (void**)&L.lvl, (MAXK + 1) * 8))) return rc;
+    if ((rc = lane_alloc(ls, (void**)&L.qel, 8))) return rc;
+    const uint64_t ntiles = cap / WS_ROWS + 2;
+    if ((rc = lane_alloc(ls, (void**)&L.status, ntiles * 8))) return rc;
+    MG_CK(cudaMemset(L.status, 0, ntiles * 8));
+    if ((rc = lane_alloc(ls, (void**)&L.tile_row, (ls->seg_cap / EXPAND_BLOCK + 2) * 4))) return rc;
+    for (uint32_t l = 0; l < ls->kmax; ++l) {
+      const uint64_t rows = l == 0 ? 1 : cap;
+      for (uint32_t j = 0; j < l; ++j)
+        if ((rc = lane_alloc(ls, (void**)&L.col[l][j], rows * 4))) return rc;
+      if ((rc = lane_alloc(ls, (void**)&L.work[l], rows * 4))) return rc;
+      if ((rc = lane_alloc(ls, (void**)&L.woff[l], (rows + 1) * 8))) return rc;
+      if ((rc = lane_alloc(ls, (void**)&L.dstart[l], rows * 4))) return rc;
+      if ((rc = lane_alloc(ls, (void**)&L.dci[l], rows))) return rc;
+    }
+  }
+  return MG_OK;
+}
+
+// Last level a plan expands in count mode: k-1, or k-2 when the last
+// position is closed in place, or k-3 when a pendant tail is closed from
+// dense aggregates.
+static int last_level(const PlanDev& P, bool dense) {
+  int l = int(P.k) - 1;
+  if (P.k >= 2 && P.last_o1) l = int(P.k) - 2;
+  if (dense && P.tail2) l = int(P.k) - 3;
+  return l;
+}
+
+static int subiso_batch_lanes(DevGraph* dg, std::vector<PlanDev>& plans, const mg_opts& o,
+                              uint64_t* counts_out, uint64_t* level_rows_out, RunResult* res) {
+  const uint32_t nq = uint32_t(plans.size());
+  uint32_t kmax = 1;
+  for (auto& p : plans) kmax = std::max(kmax, p.k);
+  const uint32_t nl = o.lanes ? o.lanes : kLanes;
+  if (nl > 64) return set_error(MG_E_ARG, "lanes=%u: at most 64", nl);
+  uint64_t cap = o.chunk_rows ? o.chunk_rows : kLaneCap;
+  if (cap > (1ull << 31)) return set_error(MG_E_ARG, "chunk_rows above 2^31");
+  int rc = ensure_lanes(dg, nl, cap, kmax);
+  if (rc) return rc;
+  LaneSet* ls = dg->lanes;
+  cudaStream_t st = dg->stream;
+  const unsigned sms = dg->sms;
+
+  // Dense pendant-tail aggregates for the batch's tail keys, while they fit
+  // 2^27 entries; plans whose key does not fit expand their tail instead.
+  std::vector<TailKey> keys;
+  uint64_t dense_entries = 0;
+  if (o.no_tail != 1) {
+    for (PlanDev& p : plans) {
+      if (!p.tail2) continue;
+      TailKey tk{p.tail_da, p.label[p.k - 2], p.tail_db, p.label[p.k - 1], p.label[p.tail_p], 0,
+                 0};
+      uint32_t kid = 0;
+      while (kid < keys.size() && std::memcmp(&keys[kid], &tk, 24) != 0) ++kid;
+      if (kid == keys.size()) {
+        const uint64_t nb = dg->h_bucket_off[tk.lp + 1] - dg->h_bucket_off[tk.lp];
+        if (dense_entries + nb > (1ull << 27)) {
+          p.tail2 = 0;
+          continue;
+        }
+        tk.base = dense_entries;
+        dense_entries += nb;
+        keys.push_back(tk);
+      }
+      p.tail_kid = kid;
+    }
+  } else {
+    for (PlanDev& p : plans) p.tail2 = 0;
+  }
+  if (ls->td_cap < dense_entries) {
+    if ((rc = lane_alloc(ls, (void**)&ls->tdA, dense_entries * 8))) return rc;
+    if ((rc = lane_alloc(ls, (void**)&ls->tdAD, dense_entries * 8))) return rc;
+    ls->td_cap = dense_entries;
+  }
+  if (ls->tkeys_cap < keys.size()) {
+    if ((rc = lane_alloc(ls, (void**)&ls->tkeys, keys.size() * sizeof(TailKey)))) return rc;
+    ls->tkeys_cap = uint32_t(keys.size());
+  }
+  if (ls->plans_cap < nq) {
+    if ((rc = lane_alloc(ls, (void**)&ls->plans, uint64_t(nq) * sizeof(PlanDev)))) return rc;
+    ls->plans_cap = nq;
+  }
+  if (ls->r_cap < nq) {
+    if ((rc = lane_alloc(ls, (void**)&ls->r_counts, uint64_t(nq) * 8))) return rc;
+    if ((rc = lane_alloc(ls, (void**)&ls->r_lvl, uint64_t(nq) * (MAXK + 1) * 8))) return rc;
+    if ((rc = lane_alloc(ls, (void**)&ls->r_err, uint64_t(nq) * 8))) return rc;
+    ls->r_cap = nq;
+  }
+  Workspace* ws = dg->ws;  // timing events live with the graph's workspace
+  if (!ws && (rc = ensure_ws(dg, 1ull << 16, 1, 1))) return rc;
+  ws = dg->ws;
+  MG_CK(cudaEventRecord(ws->ev0, st));
+  MG_CK(cudaMemcpyAsync(ls->plans, plans.data(), uint64_t(nq) * sizeof(PlanDev),
+                        cudaMemcpyHostToDevice, st));
+  if (!keys.empty()) {
+    MG_CK(cudaMemcpyAsync(ls->tkeys, keys.data(), keys.size() * sizeof(TailKey),
+                          cudaMemcpyHostToDevice, st));
+    for (const TailKey& tk : keys) {
+      const uint32_t nb = dg->h_bucket_off[tk.lp + 1] - dg->h_bucket_off[tk.lp];
+      if (!nb) continue;
+      k_tail_dense<<<grid_for(uint64_t(nb) * 32, 256, sms * 16), 256, 0, st>>>(dg->g, tk, nb,
+                                                                             ls->tdA, ls->tdAD);
+      res->launches++;
+    }
+  }
+  MG_CK(cudaEventRecord(ls->ev_start, st));
+
+  StepArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.g = dg->g;
+  a.count_mode = 1;
+  a.filters = o.filters & MG_FILTER_ALL;
+  a.grab = o.grab;
+  a.root_step = 1;
+  a.probe_min = o.probe_min ? o.probe_min : kProbeMin;
+  a.q_budget = o.max_elements;
+  a.lane = 1;
+  a.cap_rows = cap;
+  a.seg_cap = ls->seg_cap;
+  a.spin_limit = kSpinLimit;
+  a.nq = 1;
+  a.tail_dense = keys.empty() ? 0u : 1u;
+  a.tdA = ls->tdA;
+  a.tdAD = ls->tdAD;
+  a.tkeys = ls->tkeys;
+  for (Lane& L : ls->lanes) {
+    MG_CK(cudaStreamWaitEvent(L.st, ls->ev_start, 0));
+    MG_CK(cudaMemsetAsync(L.ctr, 0, C_NUM * 8, L.st));
+    MG_CK(cudaMemsetAsync(L.counts, 0, 8, L.st));
+    MG_CK(cudaMemsetAsync(L.lvl, 0, (MAXK + 1) * 8, L.st));
+    MG_CK(cudaMemsetAsync(L.qel, 0, 8, L.st));
+  }
+  const unsigned g_ws = sms * 2, g_tr = sms * 2, g_ex = sms * 4;
+  for (uint32_t j = 0; j < nq; ++j) {
+    Lane& L = ls->lanes[j % nl];
+    const PlanDev& P = plans[j];
+    a.plans = ls->plans + j;
+    a.ctr = L.ctr;
+    a.counts = L.counts;
+    a.lvl_rows = L.lvl;
+    a.q_elems = L.qel;
+    a.scan_status = L.status;
+    a.tile_row = L.tile_row;
+    const int last = P.zero ? -1 : last_level(P, a.tail_dense != 0);
+    for (int l = 0; l <= last; ++l) {
+      a.level = uint32_t(l);
+      TabPtrs t{};
+      for (int c = 0; c < l; ++c) t.col[c] = L.col[l][c];
+      a.in = t;
+      a.work = L.work[l];
+      a.woff = L.woff[l];
+      a.dstart = L.dstart[l];
+      a.dci = L.dci[l];
+      if (++L.epoch > kEpochMax) {
+        MG_CK(cudaMemsetAsync(L.status, 0, (cap / WS_ROWS + 2) * 8, L.st));
+        L.epoch = 1;
+      }
+      k_work_scan<<<g_ws, 256, 0, L.st>>>(a, L.epoch);
+      k_tile_rows_lane<<<g_tr, 256, 0, L.st>>>(a);
+      const bool writes = l < last;
+      TabPtrs out{};
+      if (writes)
+        for (int c = 0; c <= l; ++c) out.col[c] = L.col[l + 1][c];
+      a.out = out;
+      a.out_cap = writes ? cap : 0;
+      a.out_slot = C_LOUT + l;
+      a.tile_slot = C_LTILE + l;
+      launch_expand(a, &P, 1, true, writes, g_ex, L.st);
+      res->launches += 3;
+      res->expand_launches++;
+    }
+    k_lane_done<<<1, 32, 0, L.st>>>(L.ctr, L.counts, L.lvl, L.qel, o.max_elements, j,
+                                   ls->r_counts, ls->r_lvl, ls->r_err);
+    res->launches++;
+  }
+  MG_CK(cudaGetLastError());
+  for (Lane& L : ls->lanes) {
+    MG_CK(cudaEventRecord(ls->ev_end, L.st));
+    MG_CK(cudaStreamWaitEvent(st, ls->ev_end, 0));
+  }
+  MG_CK(cudaEventRecord(ws->ev1, st));
+  std::vector<unsigned long long> err(nq), cnt(nq), lv(uint64_t(nq) * (MAXK + 1));
+  std::vector<unsigned long long> lctr(uint64_t(nl) * C_NUM);
+  MG_CK(cudaMemcpyAsync(cnt.data(), ls->r_counts, uint64_t(nq) * 8, cudaMemcpyDeviceToHost, st));
+  MG_CK(cudaMemcpyAsync(err.data(), ls->r_err, uint64_t(nq) * 8, cudaMemcpyDeviceToHost, st));
+  MG_CK(cudaMemcpyAsync(lv.data(), ls->r_lvl, lv.size() * 8, cudaMemcpyDeviceToHost, st));
+  for (uint32_t l = 0; l < nl; ++l)
+    MG_CK(cudaMemcpyAsync(lctr.data() + uint64_t(l) * C_NUM, ls->lanes[l].ctr, C_NUM * 8,
+                          cudaMemcpyDeviceToHost, st));
+  MG_CK(cudaStreamSynchronize(st));
+  float ms = 0;
+  MG_CK(cudaEventElapsedTime(&ms, ws->ev0, ws->ev1));
+  res->ms = ms;
+  for (uint32_t l = 0; l < nl; ++l) {
+    res->balg += lctr[uint64_t(l) * C_NUM + C_BALG];
+    res->balgc += lctr[uint64_t(l) * C_NUM + C_BALGC];
+  }
+  for (uint32_t j = 0; j < nq; ++j) {
+    if (err[j] & ERR_TIMEOUT)
+      return set_error(MG_E_TIMEOUT, "query %u: a lane's device wait gave up", j);
+    if (err[j] & ERR_OVERFLOW) {
+      // Did not fit its lane: count it again on the chunked path.
+      std::vector<PlanDev> one(1, plans[j]);
+      RunResult r1;
+      uint64_t c1 = 0;
+      std::vector<uint64_t> l1(MAXK + 1, 0);
+      mg_opts o1 = o;
+      o1.chunk_rows = 0;
+      if ((rc = run_levels(dg, one, true, nullptr, o1, &c1, &r1, l1.data()))) return rc;
+      cnt[j] = c1;
+      for (uint32_t i = 0; i <= MAXK; ++i) lv[uint64_t(j) * (MAXK + 1) + i] = l1[i];
+      res->ms += r1.ms;
+      res->launches += r1.launches;
+      res->reruns++;
+    }
+  }
+  for (uint32_t j = 0; j < nq; ++j) counts_out[j] = cnt[j];
+  if (level_rows_out)
+    for (uint64_t x = 0; x < lv.size(); ++x) level_rows_out[x] = lv[x];
+  return MG_OK;
+}
+
 int subiso_batch(DevGraph* dg, const mg_csr_view* const* qs, uint32_t nq, const mg_opts* opts,
                  uint64_t* counts, mg_stats* st, const uint32_t* orders = nullptr,
                  uint64_t* level_rows = nullptr) {
@@ -1607,7 +2113,9 @@ int subiso_batch(DevGraph* dg, const mg_csr_view* const* qs, uint32_t nq, const 
     if (rc) return set_error(rc, "query %u: %s", i, last_error_cstr());
   }
   RunResult res;
-  int rc = run_levels(dg, plans, true, nullptr, o, counts, &res, level_rows);
+  int rc = o.lanes == MG_LANES_SHARED
+               ? run_levels(dg, plans, true, nullptr, o, counts, &res, level_rows)
+               : subiso_batch_lanes(dg, plans, o, counts, level_rows, &res);
   if (rc) return rc;
   if (st) {
     std::memset(st, 0, sizeof(*st));
@@ -1890,6 +2398,8 @@ int noalloc_count(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint6
   a.tile_row = L.tile_row;
   a.root_step = o.root_step > 1 ? o.root_step : 1u;
   a.probe_min = o.probe_min ? o.probe_min : kProbeMin;
+  a.out_slot = C_OUT;
+  a.tile_slot = C_TILE;
   if (o.root_end || a.root_step > 1) {
     a.root_begin = o.root_begin;
     a.root_end = o.root_end ? o.root_end : ~0ull;

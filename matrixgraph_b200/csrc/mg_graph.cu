@@ -35,6 +35,7 @@ int dev_alloc(DevGraph* dg, void** p, size_t bytes) {
 }
 
 void free_workspace(Workspace* ws);
+void free_lanes(LaneSet* ls);
 
 DevGraph::~DevGraph() {
   if (stream) {
@@ -43,6 +44,7 @@ DevGraph::~DevGraph() {
     cudaSetDevice(device);
     cudaStreamSynchronize(stream);
     free_workspace(ws);
+    free_lanes(lanes);
     for (void* p : allocs) cudaFree(p);
     cudaStreamDestroy(stream);
     cudaSetDevice(prev);

@@ -33,7 +33,7 @@ ORDERS = {"reference": L.MG_ORDER_REFERENCE, "heuristic": L.MG_ORDER_REFERENCE,
 
 def make_opts(order="reference", filters=L.MG_FILTER_ALL, chunk_rows=0, given_order=None,
               model=None, root_range=None, mem_budget_bytes=0, root_step=0,
-              grab=0, no_tail=0, max_elements=0, probe_min=0, kernel_events=0):
+              grab=0, no_tail=0, max_elements=0, probe_min=0, kernel_events=0, lanes=0):
     o = L.default_opts()
     o.no_tail = no_tail
     o.max_elements = max_elements
@@ -44,6 +44,7 @@ def make_opts(order="reference", filters=L.MG_FILTER_ALL, chunk_rows=0, given_or
     o.root_step = root_step
     o.probe_min = probe_min
     o.kernel_events = kernel_events
+    o.lanes = L.MG_LANES_SHARED if lanes == "shared" else int(lanes)
     o.grab = grab
     keep = None
     if given_order is not None:

@@ -380,3 +380,33 @@ def test_hub_bitmaps_never_change_results(directed):
     finally:
         for dg in handles.values():
             dg.free()
+
+
+def test_batch_lane_pipeline_variants(c1):
+    """The lane pipeline (sizes on the device, one host wait per batch) gives
+    the per-query counts and prefix survivors for any lane count, with lane
+    tables so small that most queries overflow and are counted again on the
+    chunked path, and agrees with the level-synchronous shared-table run."""
+    g, q, dg = c1
+    rng = np.random.default_rng(21)
+    qs = [mg.query_random(g, 3 + i % 6, 0.3, seed=5000 + i) for i in range(48)]
+    qs += [mg.query_walk(g, s, seed=70 + i) for i, s in enumerate(mg.SHAPES)]
+    single = [dg.count(x) for x in qs]
+    orders = [mg.plan_order(x) for x in qs]
+    _, ref_rows, _ = dg.batch_count_orders(qs, orders, lanes="shared")
+    for lanes in (1, 3, 0):
+        for chunk in (0, 64):
+            got, st = dg.batch_count(qs, stats=True, lanes=lanes, chunk_rows=chunk)
+            assert got.tolist() == single, (lanes, chunk)
+            assert st["device_ms"] > 0
+            counts, rows, _ = dg.batch_count_orders(qs, orders, lanes=lanes, chunk_rows=chunk)
+            assert counts.tolist() == single
+            assert rows.tolist() == ref_rows.tolist(), (lanes, chunk)
+    assert dg.batch_count(qs, lanes="shared").tolist() == single
+    for x, c in list(zip(qs, single))[::7]:
+        assert oracle_count(g, x)["count"] == c
+    # pendant tails closed from dense aggregates inside the lanes, and without
+    tq = [mg.CSRGraph.query(k, qe, rng.integers(0, 8, k).tolist()) for k, qe in TAIL_QUERIES]
+    ref = [dg.count(x, no_tail=1) for x in tq]
+    assert dg.batch_count(tq).tolist() == ref
+    assert dg.batch_count(tq, no_tail=1).tolist() == ref
