@@ -26,8 +26,7 @@ constexpr uint32_t ERR_TIMEOUT = 4u;    // a bounded device wait gave up
 //   nlb[d]   : n*W neighbour-label bits (bit l: v has a d-neighbour labelled l)
 //   deg[d]   : distinct d-neighbours
 //   label    : compact labels 0..L-1
-//   bucket_* : vertices grouped by label (ascending id inside a bucket);
-//              bucket_pos[v] = index of v inside its bucket
+//   bucket_* : vertices grouped by label (ascending id inside a bucket)
 //   selfbits : bit v set when (v, v) is an edge
 //   globalid : local id -> global id of the reference format
 struct GraphDev {
@@ -39,7 +38,6 @@ struct GraphDev {
   const uint32_t* label;
   const uint32_t* bucket_off;
   const uint32_t* bucket_vid;
-  const uint32_t* bucket_pos;  // position of every vertex inside its label bucket
   const uint32_t* selfbits;
   const uint32_t* globalid;
   // Hub bitmaps per direction (nullptr: none): hub_slot[d][v] is v's row in
@@ -47,6 +45,8 @@ struct GraphDev {
   // d-neighbour of v.
   const uint16_t* hub_slot[2];
   const uint32_t* hub_bits[2];
+  const uint32_t* hub_vid[2];  // vertex of each hub slot
+  uint32_t n_hubs[2];
   uint32_t hub_words;
 };
 constexpr uint16_t NO_HUB = 0xFFFF;
@@ -81,13 +81,13 @@ struct PlanDev {
 };
 
 // Signature of a two-hop aggregate: A(y) = sum over the da-slice of y labelled
-// la of the db-slice lengths labelled lb.  Queries sharing a signature share
-// memoised aggregates.
+// la of the db-slice lengths labelled lb.  Queries of one call sharing a
+// signature share the hub table of aggregates.
 struct TailKey {
   uint32_t da, la, db, lb;
-  uint32_t lp;     // label of m_p (dense aggregates cover this label's bucket)
+  uint32_t lp;     // label of m_p: only hubs with this label get aggregates
   uint32_t pad;
-  uint64_t base;   // first entry of this key in the dense aggregate arrays
+  uint64_t base;   // first entry of this key's hub table (~0: none, sum in place)
 };
 
 struct Workspace;  // enumeration scratch (mg_enum.cu)

@@ -38,6 +38,15 @@ const char* last_error_cstr();
 // ---------------------------------------------------------------------------
 // Workspace (per graph handle)
 // ---------------------------------------------------------------------------
+// Pendant-tail keys of a call and the two-hop aggregates of their hubs.
+struct TailStore {
+  unsigned long long* A = nullptr;
+  unsigned long long* AD = nullptr;
+  uint64_t cap = 0;
+  TailKey* keys = nullptr;
+  uint32_t keys_cap = 0;
+};
+
 struct Workspace {
   int device = 0;
   uint64_t cap = 0;       // rows per level table (and elements per chunk)
@@ -52,18 +61,7 @@ struct Workspace {
   uint64_t* bsum = nullptr;
   uint32_t bsum_cap = 0;
   uint32_t* tile_row = nullptr;  // first row of every expand tile of a segment
-  // Memoised two-hop aggregates: open-addressing table keyed by
-  // (tail key id << 32 | vertex), values A and AD, list of new slots.
-  uint64_t* hkeys = nullptr;
-  unsigned long long* hA = nullptr;
-  unsigned long long* hAD = nullptr;
-  uint32_t* hnew = nullptr;
-  uint64_t hsize = 0;
-  TailKey* tkeys = nullptr;
-  uint32_t tkeys_cap = 0;
-  unsigned long long* tdA = nullptr;   // dense aggregates (tail keys' buckets)
-  unsigned long long* tdAD = nullptr;
-  uint64_t td_cap = 0;
+  TailStore tails;
   unsigned long long* ctr = nullptr;     // device counters
   unsigned long long* h_ctr = nullptr;   // pinned mirror
   unsigned long long* counts = nullptr;  // per query
@@ -79,7 +77,7 @@ struct Workspace {
 
 // Counter slots.
 enum : int {
-  C_OUT = 0, C_BALG = 1, C_BALGC = 2, C_ERR = 3, C_EMIT = 4, C_HNEW = 5, C_TILE = 6,
+  C_OUT = 0, C_BALG = 1, C_BALGC = 2, C_ERR = 3, C_EMIT = 4, C_TILE = 6,
   // Lane pipeline (sizes live on the device), one slot per level l:
   C_LOUT = 8,                // rows the expand of level l wrote (= rows of level l+1)
   C_LTILE = C_LOUT + MAXK,   // work-queue position of the expand of level l
@@ -203,17 +201,11 @@ struct StepArgs {
   uint32_t root_step;             // level-0 stride inside the range (>= 1)
   uint32_t probe_min;             // shortest hub slice probed in the hub bitmap
   const uint32_t* tile_row;        // first row of each tile of [t0, t1)
-  // Pendant tails counted in closed form (tail_on): memo table of aggregates.
   uint32_t grab;   // expand tiles taken per work-queue grab
-  uint32_t tail_on;
-  uint64_t* hkeys;
-  unsigned long long* hA;
-  unsigned long long* hAD;
-  uint32_t* hnew;
-  uint64_t hmask;
   const TailKey* tkeys;
-  // Dense two-hop aggregates (tail_dense): entry tkeys[kid].base +
-  // bucket_pos[m_p]; the tail is then counted while expanding position k-3.
+  // Two-position pendant tails (tail_dense): counted while expanding
+  // position k-3; the two-hop aggregates of a hub m_p are read at
+  // tkeys[kid].base + hub slot, those of other vertices summed in place.
   uint32_t tail_dense;
   const unsigned long long* tdA;
   const unsigned long long* tdAD;
@@ -328,33 +320,6 @@ __device__ __forceinline__ uint32_t find_row(const uint64_t* __restrict__ woff, 
   return lo;
 }
 
-// Memo table of two-hop aggregates (open addressing, linear probing).  The
-// host keeps the load at or below one half, so probing always ends.
-constexpr uint64_t MEMO_EMPTY = ~0ull;
-
-__device__ __forceinline__ uint64_t memo_hash(uint64_t key) {
-  key ^= key >> 33;
-  key *= 0xff51afd7ed558ccdull;
-  key ^= key >> 33;
-  key *= 0xc4ceb9fe1a85ec53ull;
-  key ^= key >> 33;
-  return key;
-}
-
-__device__ __forceinline__ uint64_t memo_find(const StepArgs& a, uint64_t key) {
-  uint64_t slot = memo_hash(key) & a.hmask;
-  for (uint64_t probe = 0; probe <= a.hmask; ++probe) {
-    const uint64_t k = a.hkeys[slot];
-    if (k == key || k == MEMO_EMPTY) break;
-    slot = (slot + 1) & a.hmask;
-  }
-  return slot;
-}
-
-__device__ __forceinline__ bool tail_row(const StepArgs& a, const PlanDev& P) {
-  return a.tail_on && P.tail2 && a.level + 2 == P.k;
-}
-
 // Adds a thread's accumulated match count and prefix survivors of query q:
 // s1 prefixes of length i+1, s2 of length i+2 and sk of length k (the last
 // two from closed-form counts).
@@ -387,46 +352,22 @@ __device__ __forceinline__ void acc_flush_warp(const StepArgs& a, uint32_t q, ui
   }
 }
 
-// Inserts (tail key, m_p) of every tail row; new slots are listed in hnew.
-__global__ void __launch_bounds__(256) k_tail_collect(StepArgs a) {
-  for (uint64_t r = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; r < a.R;
-       r += uint64_t(gridDim.x) * blockDim.x) {
-    const uint32_t q = a.in.qid ? a.in.qid[r] : 0u;
-    const PlanDev& P = a.plans[q];
-    if (!tail_row(a, P)) continue;
-    const uint64_t key = (uint64_t(P.tail_kid) << 32) | a.in.col[P.tail_p][r];
-    uint64_t slot = memo_hash(key) & a.hmask;
-    for (uint64_t probe = 0; probe <= a.hmask; ++probe) {
-      const uint64_t seen = a.hkeys[slot];  // plain probe first: most keys exist
-      if (seen == key) break;
-      if (seen != MEMO_EMPTY) {
-        slot = (slot + 1) & a.hmask;
-        continue;
-      }
-      const unsigned long long old = atomicCAS(
-          reinterpret_cast<unsigned long long*>(a.hkeys + slot), MEMO_EMPTY, key);
-      if (old == MEMO_EMPTY) {
-        const unsigned long long idx = atomicAdd(&a.ctr[C_HNEW], 1ull);
-        a.hnew[idx] = uint32_t(slot);
-        break;
-      }
-      if (old == key) break;
-      slot = (slot + 1) & a.hmask;
-    }
-  }
-}
-
-// Dense aggregates of one tail key over the whole label bucket of m_p, warp
-// per bucket position: tdA[base + j], tdAD[base + j] for y = bucket_vid[j].
-__global__ void __launch_bounds__(256) k_tail_dense(GraphDev g, TailKey tk, uint32_t nb,
+// Two-hop aggregates of one tail key for the hubs of direction da, warp per
+// hub: for y labelled lp,
+//   A(y)  = sum_{x in N^{da}_{la}(y)} (|N^{db}_{lb}(x)| - [x self-loop, la == lb]),
+//   AD(y) = sum_{x in N^{da}_{la}(y)} |N^{db}_{lb}(x)|
+// at tdA / tdAD[tk.base + hub slot] (hubs of other labels are skipped: no
+// prefix can match them at position p).
+__global__ void __launch_bounds__(256) k_tail_dense(GraphDev g, TailKey tk,
                                                     unsigned long long* tdA,
                                                     unsigned long long* tdAD) {
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t warp = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5;
   const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-  const uint32_t b0 = __ldg(g.bucket_off + tk.lp);
-  for (uint64_t j = warp; j < nb; j += nwarps) {
-    const uint32_t y = __ldg(g.bucket_vid + b0 + j);
+  const uint32_t nh = g.n_hubs[tk.da];
+  for (uint64_t h = warp; h < nh; h += nwarps) {
+    const uint32_t y = __ldg(g.hub_vid[tk.da] + h);
+    if (__ldg(g.label + y) != tk.lp) continue;
     uint32_t s, e;
     slice_of(g, tk.da, y, tk.la, s, e);
     unsigned long long sa = 0, sd = 0;
@@ -440,48 +381,39 @@ __global__ void __launch_bounds__(256) k_tail_dense(GraphDev g, TailKey tk, uint
     sa = warp_sum(sa);
     sd = warp_sum(sd);
     if (lane == 0) {
-      tdA[tk.base + j] = sa;
-      tdAD[tk.base + j] = sd;
+      tdA[tk.base + h] = sa;
+      tdAD[tk.base + h] = sd;
     }
   }
 }
 
-// Aggregates of the new slots, warp per slot:
-// A(y) = sum_{x in N^{da}_{la}(y)} (|N^{db}_{lb}(x)| - [x self-loop, la == lb]),
-// AD(y) = sum_{x in N^{da}_{la}(y)} |N^{db}_{lb}(x)|.
-__global__ void __launch_bounds__(256) k_tail_compute(StepArgs a, uint64_t first) {
+// Two-hop aggregates A(m_p), AD(m_p) of a tail (see k_tail_dense): from the
+// hub table when m_p is a hub, else summed over its label-l_a slice [s, e),
+// which is short for a vertex below the hub degree.
+__device__ __forceinline__ void tail_agg(const StepArgs& a, const PlanDev& P, uint32_t mp,
+                                         uint32_t s, uint32_t e, long long& c, long long& d) {
   const GraphDev& g = a.g;
-  const uint32_t lane = threadIdx.x & 31;
-  const uint64_t warp = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5;
-  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-  const uint64_t total = a.ctr[C_HNEW];
-  for (uint64_t w = first + warp; w < total; w += nwarps) {
-    const uint32_t slot = a.hnew[w];
-    const uint64_t key = a.hkeys[slot];
-    const TailKey tk = a.tkeys[key >> 32];
-    const uint32_t y = uint32_t(key);
-    uint32_t s, e;
-    slice_of(g, tk.da, y, tk.la, s, e);
-    unsigned long long sa = 0, sd = 0;
-    for (uint32_t j = s + lane; j < e; j += 32) {
-      const uint32_t x = __ldg(g.adj[tk.da] + j);
-      uint32_t xs, xe;
-      slice_of(g, tk.db, x, tk.lb, xs, xe);
-      sd += xe - xs;
-      sa += xe - xs - ((tk.la == tk.lb && has_self(g, x)) ? 1u : 0u);
+  const uint32_t da = P.tail_da, db = P.tail_db;
+  const TailKey& tk = a.tkeys[P.tail_kid];
+  if (tk.base != ~0ull && g.hub_slot[da]) {
+    const uint16_t h = __ldg(g.hub_slot[da] + mp);
+    if (h != NO_HUB) {
+      c = (long long)a.tdA[tk.base + h];
+      d = (long long)a.tdAD[tk.base + h];
+      return;
     }
-    sa = warp_sum(sa);
-    sd = warp_sum(sd);
-    if (lane == 0) {
-      a.hA[slot] = sa;
-      a.hAD[slot] = sd;
-    }
+  }
+  const uint32_t la = tk.la, lb = tk.lb;
+  c = d = 0;
+  for (uint32_t j = s; j < e; ++j) {
+    const uint32_t x = __ldg(g.adj[da] + j);
+    uint32_t xs, xe;
+    slice_of(g, db, x, lb, xs, xe);
+    d += xe - xs;
+    c += (long long)(xe - xs) - ((la == lb && has_self(g, x)) ? 1 : 0);
   }
 }
 
-// Work kernel: per row, the driving slice (shortest backward slice, or the
-// label bucket for a position without backward neighbours) and the
-// algorithmic-byte charge of extending the row.
 // Closed-form count of one prefix of length a = k-2 under a two-position
 // pendant tail (PlanDev::tail2).  With I the matched prefix, S = the
 // label-l_a slice [s, e) of m_p, D(x) = |N_{l_b}(x)| and c(x) = D(x) - [x has
@@ -522,18 +454,6 @@ __device__ __forceinline__ void tail_close(const StepArgs& a, const PlanDev& P, 
   cnt = (unsigned long long)c;
   pre = (unsigned long long)(e - s) - inS;
   dsum = (unsigned long long)d;
-}
-
-// Tail count of table row r from the memoised aggregates.
-__device__ __forceinline__ void tail_count(const StepArgs& a, const PlanDev& P, uint64_t r,
-                                           unsigned long long& cnt, unsigned long long& pre,
-                                           unsigned long long& dsum) {
-  const uint32_t mp = a.in.col[P.tail_p][r];
-  uint32_t s, e;
-  slice_of(a.g, P.tail_da, mp, P.label[P.k - 2], s, e);
-  const uint64_t slot = memo_find(a, (uint64_t(P.tail_kid) << 32) | mp);
-  tail_close(a, P, [&](uint32_t j) { return a.in.col[j][r]; }, mp, s, e,
-             (long long)a.hA[slot], (long long)a.hAD[slot], cnt, pre, dsum);
 }
 
 // Work kernel: per row, the driving slice (shortest backward slice, or the
@@ -592,48 +512,18 @@ __device__ __forceinline__ uint32_t row_work(const StepArgs& a, const PlanDev& P
 }
 
 __global__ void __launch_bounds__(256) k_work(StepArgs a) {
-  unsigned long long bal = 0, balc = 0, tcnt = 0, tpre = 0;
-  uint32_t tq = 0;
-  const uint32_t i = a.level;
-  const GraphDev& g = a.g;
-  // Contiguous rows per block: rows of one query stay together, so the
-  // per-thread tail-count accumulator rarely changes query.
+  unsigned long long bal = 0, balc = 0;
+  // Contiguous rows per block: rows of one query stay together.
   const uint64_t per = ((a.R + gridDim.x - 1) / gridDim.x + blockDim.x - 1) / blockDim.x *
                        blockDim.x;
   const uint64_t r_end = min(uint64_t(a.R), (uint64_t(blockIdx.x) + 1) * per);
   for (uint64_t r = blockIdx.x * per + threadIdx.x; r < r_end; r += blockDim.x) {
     const uint32_t q = a.in.qid ? a.in.qid[r] : 0u;
     const PlanDev& P = a.plans[q];
-    const uint32_t lab = P.label[i];
-    uint32_t best, bs = 0;
-    uint8_t bci = DCI_BUCKET;
-    unsigned long long ch = 0, chc = 0;
-    if (tail_row(a, P)) {
-      // position a = k-2: one backward slice; position b counted in closed form
-      const uint32_t cs = P.cons[i][0];
-      uint32_t s, e;
-      slice_of(g, cs >> 8, a.in.col[cs & 0xFF][r], lab, s, e);
-      unsigned long long cnt, pre, dsum;
-      tail_count(a, P, r, cnt, pre, dsum);
-      ch = 8ull + 4ull * (e - s) + 8ull * pre + 4ull * dsum;
-      chc = 8ull + 4ull * (e - s) + 8ull * pre;
-      if (q != tq) {
-        acc_flush(a, tq, i, tcnt, tpre, 0);  // P_{k-1} at i+1, P_k via counts below
-        if (tcnt) atomicAdd(&a.lvl_rows[uint64_t(tq) * (MAXK + 1) + i + 2], tcnt);
-        tcnt = tpre = 0;
-        tq = q;
-      }
-      tcnt += cnt;
-      tpre += pre;
-      a.work[r] = 0;
-      a.dstart[r] = 0;
-      a.dci[r] = 0;
-      bal += ch;
-      balc += chc;
-      continue;
-    }
-    best = row_work(a, P, r, q, bs, bci, ch, chc);
-    a.work[r] = best;
+    uint32_t bs;
+    uint8_t bci;
+    unsigned long long ch, chc;
+    a.work[r] = row_work(a, P, r, q, bs, bci, ch, chc);
     a.dstart[r] = bs;
     a.dci[r] = bci;
     bal += ch;
@@ -644,18 +534,6 @@ __global__ void __launch_bounds__(256) k_work(StepArgs a) {
   if ((threadIdx.x & 31) == 0 && (bal | balc)) {
     atomicAdd(&a.ctr[C_BALG], bal);
     atomicAdd(&a.ctr[C_BALGC], balc);
-  }
-  if (a.tail_on) {
-    const bool uniform = __all_sync(FULL, tq == __shfl_sync(FULL, tq, 0));
-    unsigned long long c = tcnt, p = tpre;
-    if (uniform) {
-      c = warp_sum(tcnt);
-      p = warp_sum(tpre);
-    }
-    if (!uniform || (threadIdx.x & 31) == 0) {
-      acc_flush(a, tq, i, c, p, 0);
-      if (c) atomicAdd(&a.lvl_rows[uint64_t(tq) * (MAXK + 1) + i + 2], c);
-    }
   }
 }
 
@@ -867,10 +745,11 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
             const uint32_t mp = P.tail_p == i ? x : a.in.col[P.tail_p][r];
             uint32_t ts, te;
             slice_of(g, P.tail_da, mp, P.label[P.k - 2], ts, te);
-            const uint64_t idx = a.tkeys[P.tail_kid].base + __ldg(g.bucket_pos + mp);
+            long long ac, ad;
+            tail_agg(a, P, mp, ts, te, ac, ad);
             unsigned long long tc, tp, td;
             tail_close(a, P, [&](uint32_t j) { return j == i ? x : a.in.col[j][r]; }, mp, ts, te,
-                       (long long)a.tdA[idx], (long long)a.tdAD[idx], tc, tp, td);
+                       ac, ad, tc, tp, td);
             cnt += tc;
             sk += tc;
             s2 += tp;
@@ -1282,6 +1161,55 @@ static void launch_expand(const StepArgs& a, const PlanDev* plans, uint32_t npla
   }
 }
 
+// Tail keys (da, la, db, lb, lp) of the plans that end in a two-position
+// pendant tail, their hub aggregate tables (one entry per hub of direction
+// da; all keys of a call share one array, at most 2^27 entries — a key past
+// that sums every m_p in place) and the tail fields of `a`.
+template <class Alloc>
+static int setup_tails(DevGraph* dg, std::vector<PlanDev>& plans, TailStore& ts, Alloc alloc,
+                       cudaStream_t st, StepArgs* a, uint64_t* launches) {
+  std::vector<TailKey> keys;
+  uint64_t entries = 0;
+  for (PlanDev& p : plans) {
+    if (!p.tail2) continue;
+    TailKey tk{p.tail_da, p.label[p.k - 2], p.tail_db, p.label[p.k - 1], p.label[p.tail_p], 0, 0};
+    uint32_t kid = 0;
+    while (kid < keys.size() && std::memcmp(&keys[kid], &tk, 20) != 0) ++kid;
+    if (kid == keys.size()) {
+      const uint64_t nh = dg->g.n_hubs[tk.da];
+      tk.base = (nh && entries + nh <= (1ull << 27)) ? entries : ~0ull;
+      if (tk.base != ~0ull) entries += nh;
+      keys.push_back(tk);
+    }
+    p.tail_kid = kid;
+  }
+  if (keys.empty()) return MG_OK;
+  int rc;
+  if (ts.cap < entries) {
+    if ((rc = alloc((void**)&ts.A, entries * 8))) return rc;
+    if ((rc = alloc((void**)&ts.AD, entries * 8))) return rc;
+    ts.cap = entries;
+  }
+  if (ts.keys_cap < keys.size()) {
+    if ((rc = alloc((void**)&ts.keys, keys.size() * sizeof(TailKey)))) return rc;
+    ts.keys_cap = uint32_t(keys.size());
+  }
+  MG_CK(cudaMemcpyAsync(ts.keys, keys.data(), keys.size() * sizeof(TailKey),
+                        cudaMemcpyHostToDevice, st));
+  for (const TailKey& tk : keys) {
+    if (tk.base == ~0ull) continue;
+    k_tail_dense<<<grid_for(uint64_t(dg->g.n_hubs[tk.da]) * 32, 256, dg->sms * 16), 256, 0, st>>>(
+        dg->g, tk, ts.A, ts.AD);
+    ++*launches;
+  }
+  MG_CK(cudaGetLastError());
+  a->tail_dense = 1;
+  a->tdA = ts.A;
+  a->tdAD = ts.AD;
+  a->tkeys = ts.keys;
+  return MG_OK;
+}
+
 static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
                       const EmitBuf* emit, const mg_opts& o, uint64_t* counts_out,
                       RunResult* res, uint64_t* lvl_rows_out = nullptr) {
@@ -1357,92 +1285,16 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
 
   // Pendant tails counted in closed form (count mode): tail-key table and
   // memo table of two-hop aggregates, shared by every query of the call.
-  uint32_t tail_levels = 0;
-  uint64_t hsize_used = 0, keyspace = 0;
   bool dense = false;
   if (count_mode && o.no_tail != 1) {
-    // Tail keys (da, la, db, lb, lp): the aggregates depend on the label of
-    // m_p only through which vertices occur, so keys with different lp are
-    // kept apart for the dense layout.
-    std::vector<TailKey> keys;
-    for (PlanDev& p : plans) {
-      if (!p.tail2) continue;
-      TailKey tk{p.tail_da, p.label[p.k - 2], p.tail_db, p.label[p.k - 1], p.label[p.tail_p], 0, 0};
-      uint32_t kid = 0;
-      while (kid < keys.size() && std::memcmp(&keys[kid], &tk, sizeof(tk)) != 0) ++kid;
-      if (kid == keys.size()) {
-        keys.push_back(tk);
-        keyspace += dg->h_bucket_off[tk.lp + 1] - dg->h_bucket_off[tk.lp];
-      }
-      p.tail_kid = kid;
-      tail_levels |= 1u << (p.k - 2);
-    }
-    // Dense aggregates over whole buckets when there are few keys: each
-    // costs one pass over the bucket's la-slices, and the tail is then
-    // counted while expanding position k-3 (its rows are never stored).
-    // Otherwise aggregates are memoised for the keys that occur.
-    dense = !keys.empty() && keys.size() <= 8 && keyspace <= (1ull << 27);
-    if (dense) {
-      uint64_t base = 0;
-      for (TailKey& tk : keys) {
-        tk.base = base;
-        base += dg->h_bucket_off[tk.lp + 1] - dg->h_bucket_off[tk.lp];
-      }
-      if (ws->td_cap < base) {
-        if ((rc = ws_alloc(ws, (void**)&ws->tdA, base * 8))) return rc;
-        if ((rc = ws_alloc(ws, (void**)&ws->tdAD, base * 8))) return rc;
-        ws->td_cap = base;
-      }
-      if (ws->tkeys_cap < keys.size()) {
-        if ((rc = ws_alloc(ws, (void**)&ws->tkeys, keys.size() * sizeof(TailKey)))) return rc;
-        ws->tkeys_cap = uint32_t(keys.size());
-      }
-      MG_CK(cudaMemcpyAsync(ws->tkeys, keys.data(), keys.size() * sizeof(TailKey),
+    rc = setup_tails(dg, plans, ws->tails,
+                     [&](void** p, size_t bytes) { return ws_alloc(ws, p, bytes); }, st, &a,
+                     &res->launches);
+    if (rc) return rc;
+    dense = a.tail_dense != 0;
+    if (dense)
+      MG_CK(cudaMemcpyAsync(ws->plans, plans.data(), nq * sizeof(PlanDev),
                             cudaMemcpyHostToDevice, st));
-      MG_CK(cudaMemcpyAsync(ws->plans, plans.data(), nq * sizeof(PlanDev), cudaMemcpyHostToDevice,
-                            st));
-      for (const TailKey& tk : keys) {
-        const uint32_t nb = dg->h_bucket_off[tk.lp + 1] - dg->h_bucket_off[tk.lp];
-        if (!nb) continue;
-        k_tail_dense<<<grid_for(uint64_t(nb) * 32, 256, sms * 16), 256, 0, st>>>(
-            dg->g, tk, nb, ws->tdA, ws->tdAD);
-        res->launches++;
-      }
-      a.tail_dense = 1;
-      a.tdA = ws->tdA;
-      a.tdAD = ws->tdAD;
-      a.tkeys = ws->tkeys;
-      tail_levels = 0;
-    }
-    if (tail_levels) {
-      // Table size: twice the distinct keys that can occur (vertices of the
-      // label bucket of m_p per tail signature), at most 4 * cap slots.
-      uint64_t hs = 1024;
-      while (hs < 2 * std::min<uint64_t>(keyspace, 2 * cap)) hs <<= 1;
-      if (ws->hsize < hs) {
-        if ((rc = ws_alloc(ws, (void**)&ws->hkeys, hs * 8))) return rc;
-        if ((rc = ws_alloc(ws, (void**)&ws->hA, hs * 8))) return rc;
-        if ((rc = ws_alloc(ws, (void**)&ws->hAD, hs * 8))) return rc;
-        if ((rc = ws_alloc(ws, (void**)&ws->hnew, hs * 4))) return rc;
-        ws->hsize = hs;
-      }
-      hsize_used = hs;
-      if (ws->tkeys_cap < keys.size()) {
-        if ((rc = ws_alloc(ws, (void**)&ws->tkeys, keys.size() * sizeof(TailKey)))) return rc;
-        ws->tkeys_cap = uint32_t(keys.size());
-      }
-      MG_CK(cudaMemcpyAsync(ws->tkeys, keys.data(), keys.size() * sizeof(TailKey),
-                            cudaMemcpyHostToDevice, st));
-      MG_CK(cudaMemcpyAsync(ws->plans, plans.data(), nq * sizeof(PlanDev), cudaMemcpyHostToDevice,
-                            st));
-      MG_CK(cudaMemsetAsync(ws->hkeys, 0xFF, hsize_used * 8, st));
-      a.hkeys = ws->hkeys;
-      a.hA = ws->hA;
-      a.hAD = ws->hAD;
-      a.hnew = ws->hnew;
-      a.hmask = hsize_used - 1;
-      a.tkeys = ws->tkeys;
-    }
   }
   // writes[l]: some query can append rows to the level-(l+1) table.
   bool writes[MAXK] = {};
@@ -1452,21 +1304,7 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
           !(dense && p.tail2 && p.k == l + 3))
         writes[l] = true;
 
-  uint64_t memo_fill = 0;  // slots used in the memo table
   auto launch_work_scan = [&](int l) -> int {
-    a.tail_on = (tail_levels >> l) & 1u;
-    if (a.tail_on) {
-      // Keep the memo table at most half full: clear it when this chunk's
-      // rows could push it past that.
-      if (memo_fill + std::min<uint64_t>(R[l], keyspace) > hsize_used / 2) {
-        MG_CK(cudaMemsetAsync(ws->hkeys, 0xFF, hsize_used * 8, st));
-        MG_CK(cudaMemsetAsync(ws->ctr + C_HNEW, 0, 8, st));
-        memo_fill = 0;
-      }
-      k_tail_collect<<<grid_for(R[l], 256, sms * 16), 256, 0, st>>>(a);
-      k_tail_compute<<<grid_for(uint64_t(R[l]) * 32, 256, sms * 16), 256, 0, st>>>(a, memo_fill);
-      res->launches += 2;
-    }
     k_work<<<grid_for(R[l], 256, sms * 16), 256, 0, st>>>(a);
     const uint32_t nb = (R[l] + SCAN_TILE - 1) / SCAN_TILE;
     k_scan_reduce<<<nb, 256, 0, st>>>(ws->work[l], R[l], ws->bsum);
@@ -1474,11 +1312,7 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
     k_scan_apply<<<nb, 256, 0, st>>>(ws->work[l], R[l], ws->bsum, ws->woff[l]);
     res->launches += 4;
     MG_CK(cudaMemcpyAsync(&ws->h_ctr[0], ws->woff[l] + R[l], 8, cudaMemcpyDeviceToHost, st));
-    if (a.tail_on)
-      MG_CK(cudaMemcpyAsync(&ws->h_ctr[C_HNEW], ws->ctr + C_HNEW, 8, cudaMemcpyDeviceToHost, st));
     MG_CK(cudaStreamSynchronize(st));
-    if (a.tail_on) memo_fill = ws->h_ctr[C_HNEW];
-    a.tail_on = 0;
     return MG_OK;
   };
   auto tab = [&](int l) {
@@ -1800,10 +1634,7 @@ struct LaneSet {
   uint32_t r_cap = 0;
   PlanDev* plans = nullptr;
   uint32_t plans_cap = 0;
-  unsigned long long *tdA = nullptr, *tdAD = nullptr;
-  uint64_t td_cap = 0;
-  TailKey* tkeys = nullptr;
-  uint32_t tkeys_cap = 0;
+  TailStore tails;
   cudaEvent_t ev_start = nullptr, ev_end = nullptr;
 };
 
@@ -1900,41 +1731,6 @@ static int subiso_batch_lanes(DevGraph* dg, std::vector<PlanDev>& plans, const m
   cudaStream_t st = dg->stream;
   const unsigned sms = dg->sms;
 
-  // Dense pendant-tail aggregates for the batch's tail keys, while they fit
-  // 2^27 entries; plans whose key does not fit expand their tail instead.
-  std::vector<TailKey> keys;
-  uint64_t dense_entries = 0;
-  if (o.no_tail != 1) {
-    for (PlanDev& p : plans) {
-      if (!p.tail2) continue;
-      TailKey tk{p.tail_da, p.label[p.k - 2], p.tail_db, p.label[p.k - 1], p.label[p.tail_p], 0,
-                 0};
-      uint32_t kid = 0;
-      while (kid < keys.size() && std::memcmp(&keys[kid], &tk, 24) != 0) ++kid;
-      if (kid == keys.size()) {
-        const uint64_t nb = dg->h_bucket_off[tk.lp + 1] - dg->h_bucket_off[tk.lp];
-        if (dense_entries + nb > (1ull << 27)) {
-          p.tail2 = 0;
-          continue;
-        }
-        tk.base = dense_entries;
-        dense_entries += nb;
-        keys.push_back(tk);
-      }
-      p.tail_kid = kid;
-    }
-  } else {
-    for (PlanDev& p : plans) p.tail2 = 0;
-  }
-  if (ls->td_cap < dense_entries) {
-    if ((rc = lane_alloc(ls, (void**)&ls->tdA, dense_entries * 8))) return rc;
-    if ((rc = lane_alloc(ls, (void**)&ls->tdAD, dense_entries * 8))) return rc;
-    ls->td_cap = dense_entries;
-  }
-  if (ls->tkeys_cap < keys.size()) {
-    if ((rc = lane_alloc(ls, (void**)&ls->tkeys, keys.size() * sizeof(TailKey)))) return rc;
-    ls->tkeys_cap = uint32_t(keys.size());
-  }
   if (ls->plans_cap < nq) {
     if ((rc = lane_alloc(ls, (void**)&ls->plans, uint64_t(nq) * sizeof(PlanDev)))) return rc;
     ls->plans_cap = nq;
@@ -1949,23 +1745,22 @@ static int subiso_batch_lanes(DevGraph* dg, std::vector<PlanDev>& plans, const m
   if (!ws && (rc = ensure_ws(dg, 1ull << 16, 1, 1))) return rc;
   ws = dg->ws;
   MG_CK(cudaEventRecord(ws->ev0, st));
-  MG_CK(cudaMemcpyAsync(ls->plans, plans.data(), uint64_t(nq) * sizeof(PlanDev),
-                        cudaMemcpyHostToDevice, st));
-  if (!keys.empty()) {
-    MG_CK(cudaMemcpyAsync(ls->tkeys, keys.data(), keys.size() * sizeof(TailKey),
-                          cudaMemcpyHostToDevice, st));
-    for (const TailKey& tk : keys) {
-      const uint32_t nb = dg->h_bucket_off[tk.lp + 1] - dg->h_bucket_off[tk.lp];
-      if (!nb) continue;
-      k_tail_dense<<<grid_for(uint64_t(nb) * 32, 256, sms * 16), 256, 0, st>>>(dg->g, tk, nb,
-                                                                             ls->tdA, ls->tdAD);
-      res->launches++;
-    }
-  }
-  MG_CK(cudaEventRecord(ls->ev_start, st));
-
   StepArgs a;
   std::memset(&a, 0, sizeof(a));
+  // Pendant tails closed from hub aggregates (their table is filled on the
+  // graph's stream before the lanes start).
+  if (o.no_tail != 1) {
+    rc = setup_tails(dg, plans, ls->tails,
+                     [&](void** p, size_t bytes) { return lane_alloc(ls, p, bytes); }, st, &a,
+                     &res->launches);
+    if (rc) return rc;
+  } else {
+    for (PlanDev& p : plans) p.tail2 = 0;
+  }
+  MG_CK(cudaMemcpyAsync(ls->plans, plans.data(), uint64_t(nq) * sizeof(PlanDev),
+                        cudaMemcpyHostToDevice, st));
+  MG_CK(cudaEventRecord(ls->ev_start, st));
+
   a.g = dg->g;
   a.count_mode = 1;
   a.filters = o.filters & MG_FILTER_ALL;
@@ -1978,10 +1773,6 @@ static int subiso_batch_lanes(DevGraph* dg, std::vector<PlanDev>& plans, const m
   a.seg_cap = ls->seg_cap;
   a.spin_limit = kSpinLimit;
   a.nq = 1;
-  a.tail_dense = keys.empty() ? 0u : 1u;
-  a.tdA = ls->tdA;
-  a.tdAD = ls->tdAD;
-  a.tkeys = ls->tkeys;
   for (Lane& L : ls->lanes) {
     MG_CK(cudaStreamWaitEvent(L.st, ls->ev_start, 0));
     MG_CK(cudaMemsetAsync(L.ctr, 0, C_NUM * 8, L.st));

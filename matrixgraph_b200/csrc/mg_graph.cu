@@ -304,17 +304,18 @@ static int build_hubs(DevGraph* dg, int d, const std::vector<uint32_t>& deg, uin
   int rc;
   if ((rc = dev_alloc(dg, (void**)&d_slot, uint64_t(n) * 2))) return rc;
   if ((rc = dev_alloc(dg, (void**)&d_bits, hub_vid.size() * row_bytes))) return rc;
-  MG_CK(cudaMallocAsync((void**)&d_vid, hub_vid.size() * 4, st));
+  if ((rc = dev_alloc(dg, (void**)&d_vid, hub_vid.size() * 4))) return rc;
   MG_CK(cudaMemcpyAsync(d_slot, slot.data(), uint64_t(n) * 2, cudaMemcpyHostToDevice, st));
   MG_CK(cudaMemcpyAsync(d_vid, hub_vid.data(), hub_vid.size() * 4, cudaMemcpyHostToDevice, st));
   MG_CK(cudaMemsetAsync(d_bits, 0, hub_vid.size() * row_bytes, st));
   k_hub_bits<<<unsigned(hub_vid.size()), 256, 0, st>>>(dg->g.adj[d], dg->g.loff[d], dg->g.L,
                                                       d_vid, words, d_bits);
   MG_CK(cudaGetLastError());
-  cudaFreeAsync(d_vid, st);
   MG_CK(cudaStreamSynchronize(st));
   dg->g.hub_slot[d] = d_slot;
   dg->g.hub_bits[d] = d_bits;
+  dg->g.hub_vid[d] = d_vid;
+  dg->g.n_hubs[d] = uint32_t(hub_vid.size());
   dg->g.hub_words = words;
   dg->info.hubs += uint32_t(hub_vid.size());
   dg->info.hub_min_degree = cut;
@@ -444,19 +445,15 @@ static int upload(const mg_csr_view* v, int device, const mg_upload_opts& uo, De
   dg->stats.label_count = cnt;
   dg->h_bucket_off.assign(L + 1, 0);
   for (uint32_t l = 0; l < L; ++l) dg->h_bucket_off[l + 1] = dg->h_bucket_off[l] + uint32_t(cnt[l]);
-  std::vector<uint32_t> bvid(n), bpos(n);
+  std::vector<uint32_t> bvid(n);
   {
     std::vector<uint32_t> cur(dg->h_bucket_off.begin(), dg->h_bucket_off.end() - 1);
-    for (uint32_t i = 0; i < n; ++i) {
-      bpos[i] = cur[lab[i]] - dg->h_bucket_off[lab[i]];
-      bvid[cur[lab[i]]++] = i;
-    }
+    for (uint32_t i = 0; i < n; ++i) bvid[cur[lab[i]]++] = i;
   }
-  uint32_t *d_label, *d_boff, *d_bvid, *d_bpos, *d_self, *d_gid, *d_err;
+  uint32_t *d_label, *d_boff, *d_bvid, *d_self, *d_gid, *d_err;
   if ((rc = dev_alloc(dg, (void**)&d_label, uint64_t(n) * 4))) return rc;
   if ((rc = dev_alloc(dg, (void**)&d_boff, uint64_t(L + 1) * 4))) return rc;
   if ((rc = dev_alloc(dg, (void**)&d_bvid, uint64_t(n) * 4))) return rc;
-  if ((rc = dev_alloc(dg, (void**)&d_bpos, uint64_t(n) * 4))) return rc;
   if ((rc = dev_alloc(dg, (void**)&d_self, uint64_t((n + 31) / 32) * 4))) return rc;
   if ((rc = dev_alloc(dg, (void**)&d_gid, uint64_t(n) * 4))) return rc;
   if ((rc = dev_alloc(dg, (void**)&d_err, 16))) return rc;
@@ -464,14 +461,12 @@ static int upload(const mg_csr_view* v, int device, const mg_upload_opts& uo, De
   MG_CK(cudaMemcpyAsync(d_boff, dg->h_bucket_off.data(), uint64_t(L + 1) * 4,
                         cudaMemcpyHostToDevice, st));
   MG_CK(cudaMemcpyAsync(d_bvid, bvid.data(), uint64_t(n) * 4, cudaMemcpyHostToDevice, st));
-  MG_CK(cudaMemcpyAsync(d_bpos, bpos.data(), uint64_t(n) * 4, cudaMemcpyHostToDevice, st));
   MG_CK(cudaMemcpyAsync(d_gid, v->globalid, uint64_t(n) * 4, cudaMemcpyHostToDevice, st));
   MG_CK(cudaMemsetAsync(d_self, 0, uint64_t((n + 31) / 32) * 4, st));
   MG_CK(cudaMemsetAsync(d_err, 0, 16, st));
   dg->g.label = d_label;
   dg->g.bucket_off = d_boff;
   dg->g.bucket_vid = d_bvid;
-  dg->g.bucket_pos = d_bpos;
   dg->g.selfbits = d_self;
   dg->g.globalid = d_gid;
 
@@ -525,6 +520,8 @@ static int upload(const mg_csr_view* v, int device, const mg_upload_opts& uo, De
   if (sym) {
     dg->g.hub_slot[1] = dg->g.hub_slot[0];
     dg->g.hub_bits[1] = dg->g.hub_bits[0];
+    dg->g.hub_vid[1] = dg->g.hub_vid[0];
+    dg->g.n_hubs[1] = dg->g.n_hubs[0];
   }
   return MG_OK;
 }

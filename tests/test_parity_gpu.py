@@ -246,8 +246,9 @@ def test_subiso_exec_cli(tmp_path, c1):
     assert np.array_equal(rows.reshape(-1, 4), dg.emit(q))
 
 
-def test_tail_memo_batch_and_clearing():
-    """Memoised tail aggregates in batch mode, including memo-table clearing."""
+def test_tail_aggregates_batch_and_chunks():
+    """Pendant tails closed from hub aggregates (and summed in place for other
+    vertices) in batches and with small level chunks equal enumeration."""
     g = mg.rmat(13, n_labels=6)
     dg = mg.DeviceGraph(g)
     rng = np.random.default_rng(5)
@@ -258,8 +259,13 @@ def test_tail_memo_batch_and_clearing():
     ref = [dg.count(q, no_tail=1) for q in qs]
     assert [dg.count(q) for q in qs] == ref
     assert dg.batch_count(qs).tolist() == ref
-    # 4096-row chunks: the memo table (8192 slots) is cleared between chunks
     assert dg.batch_count(qs, chunk_rows=4096).tolist() == ref
+    assert dg.batch_count(qs, lanes="shared", chunk_rows=4096).tolist() == ref
+    # no hubs at all: every aggregate summed in place
+    dg0 = mg.DeviceGraph(g, hub_bytes=0)
+    assert [dg0.count(q) for q in qs] == ref
+    assert dg0.batch_count(qs).tolist() == ref
+    dg0.free()
     dg.free()
 
 
