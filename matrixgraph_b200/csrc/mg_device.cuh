@@ -38,6 +38,7 @@ struct GraphDev {
   const uint32_t* label;
   const uint32_t* bucket_off;
   const uint32_t* bucket_vid;
+  const uint32_t* bucket_pos;  // index of every vertex inside its label bucket
   const uint32_t* selfbits;
   const uint32_t* globalid;
   // Hub bitmaps per direction (nullptr: none): hub_slot[d][v] is v's row in
@@ -87,7 +88,9 @@ struct TailKey {
   uint32_t da, la, db, lb;
   uint32_t lp;     // label of m_p: only hubs with this label get aggregates
   uint32_t pad;
-  uint64_t base;   // first entry of this key's hub table (~0: none, sum in place)
+  uint64_t base;   // first entry of this key's hub table (~0: none)
+  uint64_t lazy;   // first entry of this key's lazily filled table over the
+                   // bucket of label lp (~0: none, sum in place)
 };
 
 struct Workspace;  // enumeration scratch (mg_enum.cu)

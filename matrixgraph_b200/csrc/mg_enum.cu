@@ -43,6 +43,8 @@ struct TailStore {
   unsigned long long* A = nullptr;
   unsigned long long* AD = nullptr;
   uint64_t cap = 0;
+  unsigned long long* lazy = nullptr;  // packed (AD << 32 | A), ~0 = not yet filled
+  uint64_t lazy_cap = 0;
   TailKey* keys = nullptr;
   uint32_t keys_cap = 0;
 };
@@ -209,6 +211,7 @@ struct StepArgs {
   uint32_t tail_dense;
   const unsigned long long* tdA;
   const unsigned long long* tdAD;
+  unsigned long long* tdL;  // lazily filled aggregates of non-hub vertices
   // Lane pipeline: row and element counts come from the counters (C_LOUT,
   // C_LT), the expand's queue and output use the per-level slots, and no
   // host value of R, t0 or t1 is read.
@@ -388,8 +391,12 @@ __global__ void __launch_bounds__(256) k_tail_dense(GraphDev g, TailKey tk,
 }
 
 // Two-hop aggregates A(m_p), AD(m_p) of a tail (see k_tail_dense): from the
-// hub table when m_p is a hub, else summed over its label-l_a slice [s, e),
-// which is short for a vertex below the hub degree.
+// hub table when m_p is a hub; otherwise from the key's lazy table over the
+// bucket of label l_p, filled on first use by whichever thread needs the
+// entry (A and AD packed in one 64-bit word, so a reader sees an entry whole
+// or not at all; concurrent fillers store the same value), or summed over the
+// label-l_a slice [s, e) when the entry cannot be tabled.  Entries whose AD
+// does not fit 32 bits are never tabled.
 __device__ __forceinline__ void tail_agg(const StepArgs& a, const PlanDev& P, uint32_t mp,
                                          uint32_t s, uint32_t e, long long& c, long long& d) {
   const GraphDev& g = a.g;
@@ -403,6 +410,16 @@ __device__ __forceinline__ void tail_agg(const StepArgs& a, const PlanDev& P, ui
       return;
     }
   }
+  unsigned long long* slot = nullptr;
+  if (tk.lazy != ~0ull) {
+    slot = a.tdL + tk.lazy + __ldg(g.bucket_pos + mp);
+    const unsigned long long w = *reinterpret_cast<volatile unsigned long long*>(slot);
+    if (w != ~0ull) {
+      c = (long long)(w & 0xFFFFFFFFull);
+      d = (long long)(w >> 32);
+      return;
+    }
+  }
   const uint32_t la = tk.la, lb = tk.lb;
   c = d = 0;
   for (uint32_t j = s; j < e; ++j) {
@@ -412,6 +429,8 @@ __device__ __forceinline__ void tail_agg(const StepArgs& a, const PlanDev& P, ui
     d += xe - xs;
     c += (long long)(xe - xs) - ((la == lb && has_self(g, x)) ? 1 : 0);
   }
+  if (slot && d < 0xFFFFFFFFll)
+    atomicExch(slot, (unsigned long long)(d) << 32 | (unsigned long long)(c));
 }
 
 // Closed-form count of one prefix of length a = k-2 under a two-position
@@ -979,7 +998,7 @@ __global__ void k_lane_done(unsigned long long* ctr, unsigned long long* counts,
                             unsigned long long* lvl, unsigned long long* qel,
                             unsigned long long budget, uint32_t q,
                             unsigned long long* out_counts, unsigned long long* out_lvl,
-                            unsigned long long* out_err) {
+                            unsigned long long* out_err, unsigned long long* out_balg) {
   const uint32_t t = threadIdx.x;
   if (t <= MAXK) {
     out_lvl[uint64_t(q) * (MAXK + 1) + t] = lvl[t];
@@ -989,9 +1008,13 @@ __global__ void k_lane_done(unsigned long long* ctr, unsigned long long* counts,
   if (t == 0) {
     out_counts[q] = (budget && qel[0] > budget) ? ~0ull : counts[0];
     out_err[q] = ctr[C_ERR];
+    out_balg[2ull * q] = ctr[C_BALG];
+    out_balg[2ull * q + 1] = ctr[C_BALGC];
     counts[0] = 0;
     qel[0] = 0;
     ctr[C_ERR] = 0;
+    ctr[C_BALG] = 0;
+    ctr[C_BALGC] = 0;
   }
   for (int c = C_LOUT + int(t); c < C_NUM; c += 32) ctr[c] = 0;
 }
@@ -1163,22 +1186,27 @@ static void launch_expand(const StepArgs& a, const PlanDev* plans, uint32_t npla
 
 // Tail keys (da, la, db, lb, lp) of the plans that end in a two-position
 // pendant tail, their hub aggregate tables (one entry per hub of direction
-// da; all keys of a call share one array, at most 2^27 entries — a key past
-// that sums every m_p in place) and the tail fields of `a`.
+// da; all keys of a call share one array of at most 2^27 entries), their lazy
+// tables over the bucket of l_p (cleared here; at most 2^30 entries in all)
+// and the tail fields of `a`.  A key past either limit sums in place.
 template <class Alloc>
 static int setup_tails(DevGraph* dg, std::vector<PlanDev>& plans, TailStore& ts, Alloc alloc,
                        cudaStream_t st, StepArgs* a, uint64_t* launches) {
   std::vector<TailKey> keys;
-  uint64_t entries = 0;
+  uint64_t entries = 0, lazy = 0;
   for (PlanDev& p : plans) {
     if (!p.tail2) continue;
-    TailKey tk{p.tail_da, p.label[p.k - 2], p.tail_db, p.label[p.k - 1], p.label[p.tail_p], 0, 0};
+    TailKey tk{p.tail_da, p.label[p.k - 2], p.tail_db, p.label[p.k - 1], p.label[p.tail_p], 0, 0,
+               0};
     uint32_t kid = 0;
     while (kid < keys.size() && std::memcmp(&keys[kid], &tk, 20) != 0) ++kid;
     if (kid == keys.size()) {
       const uint64_t nh = dg->g.n_hubs[tk.da];
       tk.base = (nh && entries + nh <= (1ull << 27)) ? entries : ~0ull;
       if (tk.base != ~0ull) entries += nh;
+      const uint64_t nb = dg->h_bucket_off[tk.lp + 1] - dg->h_bucket_off[tk.lp];
+      tk.lazy = (lazy + nb <= (1ull << 30)) ? lazy : ~0ull;
+      if (tk.lazy != ~0ull) lazy += nb;
       keys.push_back(tk);
     }
     p.tail_kid = kid;
@@ -1190,6 +1218,11 @@ static int setup_tails(DevGraph* dg, std::vector<PlanDev>& plans, TailStore& ts,
     if ((rc = alloc((void**)&ts.AD, entries * 8))) return rc;
     ts.cap = entries;
   }
+  if (ts.lazy_cap < lazy) {
+    if ((rc = alloc((void**)&ts.lazy, lazy * 8))) return rc;
+    ts.lazy_cap = lazy;
+  }
+  if (lazy) MG_CK(cudaMemsetAsync(ts.lazy, 0xFF, lazy * 8, st));
   if (ts.keys_cap < keys.size()) {
     if ((rc = alloc((void**)&ts.keys, keys.size() * sizeof(TailKey)))) return rc;
     ts.keys_cap = uint32_t(keys.size());
@@ -1206,6 +1239,7 @@ static int setup_tails(DevGraph* dg, std::vector<PlanDev>& plans, TailStore& ts,
   a->tail_dense = 1;
   a->tdA = ts.A;
   a->tdAD = ts.AD;
+  a->tdL = ts.lazy;
   a->tkeys = ts.keys;
   return MG_OK;
 }
@@ -1630,7 +1664,7 @@ struct LaneSet {
   uint32_t kmax = 0;
   std::vector<Lane> lanes;
   std::vector<void*> allocs;
-  unsigned long long *r_counts = nullptr, *r_lvl = nullptr, *r_err = nullptr;
+  unsigned long long *r_counts = nullptr, *r_lvl = nullptr, *r_err = nullptr, *r_balg = nullptr;
   uint32_t r_cap = 0;
   PlanDev* plans = nullptr;
   uint32_t plans_cap = 0;
@@ -1739,6 +1773,7 @@ static int subiso_batch_lanes(DevGraph* dg, std::vector<PlanDev>& plans, const m
     if ((rc = lane_alloc(ls, (void**)&ls->r_counts, uint64_t(nq) * 8))) return rc;
     if ((rc = lane_alloc(ls, (void**)&ls->r_lvl, uint64_t(nq) * (MAXK + 1) * 8))) return rc;
     if ((rc = lane_alloc(ls, (void**)&ls->r_err, uint64_t(nq) * 8))) return rc;
+    if ((rc = lane_alloc(ls, (void**)&ls->r_balg, uint64_t(nq) * 16))) return rc;
     ls->r_cap = nq;
   }
   Workspace* ws = dg->ws;  // timing events live with the graph's workspace
@@ -1820,7 +1855,7 @@ static int subiso_batch_lanes(DevGraph* dg, std::vector<PlanDev>& plans, const m
       res->expand_launches++;
     }
     k_lane_done<<<1, 32, 0, L.st>>>(L.ctr, L.counts, L.lvl, L.qel, o.max_elements, j,
-                                   ls->r_counts, ls->r_lvl, ls->r_err);
+                                   ls->r_counts, ls->r_lvl, ls->r_err, ls->r_balg);
     res->launches++;
   }
   MG_CK(cudaGetLastError());
@@ -1829,21 +1864,20 @@ static int subiso_batch_lanes(DevGraph* dg, std::vector<PlanDev>& plans, const m
     MG_CK(cudaStreamWaitEvent(st, ls->ev_end, 0));
   }
   MG_CK(cudaEventRecord(ws->ev1, st));
-  std::vector<unsigned long long> err(nq), cnt(nq), lv(uint64_t(nq) * (MAXK + 1));
-  std::vector<unsigned long long> lctr(uint64_t(nl) * C_NUM);
+  std::vector<unsigned long long> err(nq), cnt(nq), lv(uint64_t(nq) * (MAXK + 1)),
+      balg(uint64_t(nq) * 2);
   MG_CK(cudaMemcpyAsync(cnt.data(), ls->r_counts, uint64_t(nq) * 8, cudaMemcpyDeviceToHost, st));
   MG_CK(cudaMemcpyAsync(err.data(), ls->r_err, uint64_t(nq) * 8, cudaMemcpyDeviceToHost, st));
   MG_CK(cudaMemcpyAsync(lv.data(), ls->r_lvl, lv.size() * 8, cudaMemcpyDeviceToHost, st));
-  for (uint32_t l = 0; l < nl; ++l)
-    MG_CK(cudaMemcpyAsync(lctr.data() + uint64_t(l) * C_NUM, ls->lanes[l].ctr, C_NUM * 8,
-                          cudaMemcpyDeviceToHost, st));
+  MG_CK(cudaMemcpyAsync(balg.data(), ls->r_balg, balg.size() * 8, cudaMemcpyDeviceToHost, st));
   MG_CK(cudaStreamSynchronize(st));
   float ms = 0;
   MG_CK(cudaEventElapsedTime(&ms, ws->ev0, ws->ev1));
   res->ms = ms;
-  for (uint32_t l = 0; l < nl; ++l) {
-    res->balg += lctr[uint64_t(l) * C_NUM + C_BALG];
-    res->balgc += lctr[uint64_t(l) * C_NUM + C_BALGC];
+  for (uint32_t j = 0; j < nq; ++j) {
+    if (err[j]) continue;  // charged by its re-run below
+    res->balg += balg[2ull * j];
+    res->balgc += balg[2ull * j + 1];
   }
   for (uint32_t j = 0; j < nq; ++j) {
     if (err[j] & ERR_TIMEOUT)
@@ -1859,6 +1893,8 @@ static int subiso_batch_lanes(DevGraph* dg, std::vector<PlanDev>& plans, const m
       if ((rc = run_levels(dg, one, true, nullptr, o1, &c1, &r1, l1.data()))) return rc;
       cnt[j] = c1;
       for (uint32_t i = 0; i <= MAXK; ++i) lv[uint64_t(j) * (MAXK + 1) + i] = l1[i];
+      res->balg += r1.balg;
+      res->balgc += r1.balgc;
       res->ms += r1.ms;
       res->launches += r1.launches;
       res->reruns++;

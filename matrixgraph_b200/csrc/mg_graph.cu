@@ -445,15 +445,19 @@ static int upload(const mg_csr_view* v, int device, const mg_upload_opts& uo, De
   dg->stats.label_count = cnt;
   dg->h_bucket_off.assign(L + 1, 0);
   for (uint32_t l = 0; l < L; ++l) dg->h_bucket_off[l + 1] = dg->h_bucket_off[l] + uint32_t(cnt[l]);
-  std::vector<uint32_t> bvid(n);
+  std::vector<uint32_t> bvid(n), bpos(n);
   {
     std::vector<uint32_t> cur(dg->h_bucket_off.begin(), dg->h_bucket_off.end() - 1);
-    for (uint32_t i = 0; i < n; ++i) bvid[cur[lab[i]]++] = i;
+    for (uint32_t i = 0; i < n; ++i) {
+      bpos[i] = cur[lab[i]] - dg->h_bucket_off[lab[i]];
+      bvid[cur[lab[i]]++] = i;
+    }
   }
-  uint32_t *d_label, *d_boff, *d_bvid, *d_self, *d_gid, *d_err;
+  uint32_t *d_label, *d_boff, *d_bvid, *d_bpos, *d_self, *d_gid, *d_err;
   if ((rc = dev_alloc(dg, (void**)&d_label, uint64_t(n) * 4))) return rc;
   if ((rc = dev_alloc(dg, (void**)&d_boff, uint64_t(L + 1) * 4))) return rc;
   if ((rc = dev_alloc(dg, (void**)&d_bvid, uint64_t(n) * 4))) return rc;
+  if ((rc = dev_alloc(dg, (void**)&d_bpos, uint64_t(n) * 4))) return rc;
   if ((rc = dev_alloc(dg, (void**)&d_self, uint64_t((n + 31) / 32) * 4))) return rc;
   if ((rc = dev_alloc(dg, (void**)&d_gid, uint64_t(n) * 4))) return rc;
   if ((rc = dev_alloc(dg, (void**)&d_err, 16))) return rc;
@@ -461,12 +465,14 @@ static int upload(const mg_csr_view* v, int device, const mg_upload_opts& uo, De
   MG_CK(cudaMemcpyAsync(d_boff, dg->h_bucket_off.data(), uint64_t(L + 1) * 4,
                         cudaMemcpyHostToDevice, st));
   MG_CK(cudaMemcpyAsync(d_bvid, bvid.data(), uint64_t(n) * 4, cudaMemcpyHostToDevice, st));
+  MG_CK(cudaMemcpyAsync(d_bpos, bpos.data(), uint64_t(n) * 4, cudaMemcpyHostToDevice, st));
   MG_CK(cudaMemcpyAsync(d_gid, v->globalid, uint64_t(n) * 4, cudaMemcpyHostToDevice, st));
   MG_CK(cudaMemsetAsync(d_self, 0, uint64_t((n + 31) / 32) * 4, st));
   MG_CK(cudaMemsetAsync(d_err, 0, 16, st));
   dg->g.label = d_label;
   dg->g.bucket_off = d_boff;
   dg->g.bucket_vid = d_bvid;
+  dg->g.bucket_pos = d_bpos;
   dg->g.selfbits = d_self;
   dg->g.globalid = d_gid;
 

@@ -409,6 +409,11 @@ def test_batch_lane_pipeline_variants(c1):
             assert counts.tolist() == single
             assert rows.tolist() == ref_rows.tolist(), (lanes, chunk)
     assert dg.batch_count(qs, lanes="shared").tolist() == single
+    # algorithmic bytes do not depend on how the batch ran
+    balg = sum(dg.count(x, stats=True)[1]["balg_count_bytes"] for x in qs)
+    for lanes, chunk in ((0, 0), (3, 64), ("shared", 0)):
+        _, st = dg.batch_count(qs, stats=True, lanes=lanes, chunk_rows=chunk)
+        assert st["balg_count_bytes"] == balg, (lanes, chunk)
     for x, c in list(zip(qs, single))[::7]:
         assert oracle_count(g, x)["count"] == c
     # pendant tails closed from dense aggregates inside the lanes, and without
