@@ -248,16 +248,8 @@ __device__ __forceinline__ bool contains(const uint32_t* __restrict__ a, uint32_
   return lo < e && __ldg(a + lo) == x;
 }
 
-// Label-lab slice [s, e) of y's dir-adjacency.  The neighbour-label bit is
-// tested first: it sits in an n*W-word array that stays in L2, while the
-// n*L+1 slice offsets do not, and most (vertex, label) slices of a sparse
-// vertex are empty.
 __device__ __forceinline__ void slice_of(const GraphDev& g, uint32_t dir, uint32_t y,
                                          uint32_t lab, uint32_t& s, uint32_t& e) {
-  if (!((__ldg(g.nlb[dir] + uint64_t(y) * g.W + (lab >> 5)) >> (lab & 31)) & 1u)) {
-    s = e = 0;
-    return;
-  }
   const uint32_t* p = g.loff[dir] + uint64_t(y) * g.L + lab;
   s = __ldg(p);
   e = __ldg(p + 1);
