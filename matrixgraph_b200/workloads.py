@@ -4,6 +4,9 @@
   c=0.19), self-loops and duplicates removed, ids not permuted, 32 Zipf(1.0)
   labels: the single-query (scale 22) and batched (scale 22) data graph.
 * ``shape_queries(g)`` — the five single-query shapes with random-walk labels.
+* ``c5_graph()`` / ``c5_queries(g, n)`` — R-MAT scale 26 with 64 Zipf(1.2)
+  labels and 6-8-vertex queries (4-clique or chorded 5-cycle plus a pendant
+  path), random-walk labels.
 * batched queries — random connected queries, k uniform in 3..8, a random
   recursive spanning tree plus every other pair with probability 0.3,
   random-walk labels.  Some seeds give search spaces far beyond any time
@@ -93,6 +96,48 @@ def select_batch(dg: DeviceGraph, g, n: int = BATCH_SIZE, budget: int = BATCH_BU
     return {"graph": "rmat scale 22 (workloads.rmat_graph)", "budget_elements": budget,
             "first_seed": first_seed, "order": "reference", "seeds": seeds, "k": ks,
             "counts": counts, "elements": elements, "dropped": dropped}
+
+
+# ---- large and skewed: R-MAT scale 26 (configuration C5) ---------------------
+C5_SCALE = 26
+C5_LABELS = 64
+C5_ZIPF = 1.2
+C5_FIRST_SEED = 300000
+
+
+def c5_graph(scale: int = C5_SCALE):
+    """Symmetrised R-MAT (edge factor 16, a=0.57 b=0.19 c=0.19, self-loops and
+    repeats removed, ids not permuted) with 64 Zipf(s=1.2) labels."""
+    return rmat(scale, 16, 0.57, 0.19, 0.19, seed=0, n_labels=C5_LABELS, label_kind="zipf",
+                zipf_s=C5_ZIPF, label_seed=1)
+
+
+def c5_shape(q: int):
+    """Shape of C5 query q: k uniform in {6, 7, 8}; even q: a 4-clique plus a
+    pendant path of k-4 vertices hung from one clique vertex; odd q: a 5-cycle
+    plus one or two chords plus a pendant path of k-5 vertices hung from one
+    cycle vertex.  Drawn from numpy's PCG64 seeded with 300000 + q."""
+    rng = np.random.default_rng(C5_FIRST_SEED + q)
+    k = int(rng.integers(6, 9))
+    if q % 2 == 0:
+        core = 4
+        edges = [(a, b) for a in range(4) for b in range(a + 1, 4)]
+    else:
+        core = 5
+        edges = [(i, (i + 1) % 5) for i in range(5)]
+        chords = [(0, 2), (0, 3), (1, 3), (1, 4), (2, 4)]
+        for j in rng.choice(len(chords), size=int(rng.integers(1, 3)), replace=False):
+            edges.append(chords[int(j)])
+    prev = int(rng.integers(0, core))
+    for v in range(core, k):
+        edges.append((prev, v))
+        prev = v
+    return k, sorted((min(a, b), max(a, b)) for a, b in edges)
+
+
+def c5_queries(g, n: int, first: int = 0):
+    """C5 queries first..first+n-1 with random-walk labels (seed 300000 + q)."""
+    return [query_walk(g, c5_shape(q), seed=C5_FIRST_SEED + q) for q in range(first, first + n)]
 
 
 # ---- learned order: training and held-out queries ---------------------------
