@@ -86,6 +86,8 @@ def parse():
                    help="skip the batched-workload measurement")
     p.add_argument("--hub-bytes", type=int, default=None,
                    help="hub-bitmap budget of the upload (profiling runs; default: library)")
+    p.add_argument("--c5", type=int, default=8,
+                   help="C5 (R-MAT scale 26) queries counted after the headline (0: skip)")
     return p.parse_args()
 
 
@@ -368,6 +370,107 @@ def gar_workload(reps=3):
     return out
 
 
+def c5_workload(n_queries, oracle_check=True):
+    """Configuration C5: R-MAT scale 26 (67,108,864 vertices, ~2.1e9 directed
+    entries) with 64 Zipf(1.2) labels, queries of 6-8 vertices (4-clique or
+    chorded 5-cycle plus a pendant path).  Their reference-order counts run to
+    10^13-10^15 embeddings, so each query is counted over a strided sample of
+    its level-0 candidates: positions 0, s, 2s, ... with the smallest s (from
+    bucket/64 upward by factors of 4) whose enumeration needs at most 2^33
+    candidate elements (element counts are exact, so the sample does not
+    depend on timing).  The oracle then counts a smaller sample of two queries
+    (the first stride whose GPU count is at most 10^7) for parity, and the
+    emitted rows of a sample with at most 10^5 matches are compared whole."""
+    import numpy as np
+
+    import matrixgraph_b200 as mg
+    from matrixgraph_b200 import _lib as L
+    from matrixgraph_b200 import workloads as W
+    t0 = time.perf_counter()
+    g = W.c5_graph()
+    gen_s = time.perf_counter() - t0
+    dg = mg.DeviceGraph(g, 0)
+    upload_s = time.perf_counter() - t0 - gen_s
+    info = dg.info
+    qs = W.c5_queries(g, n_queries)
+    lab = g.array("labels")
+    sizes = np.bincount(lab, minlength=W.C5_LABELS)
+    out = {"workload": f"R-MAT scale 26 ({g.n:,} vertices, {g.m_out:,} directed entries), 64 "
+                       f"Zipf(1.2) labels; first {n_queries} C5 queries (k 6-8), reference "
+                       "order, count mode over strided root samples",
+           "gen_seconds": gen_s, "upload_seconds": upload_s,
+           "device_bytes": info["device_bytes"], "queries": []}
+    budget = 1 << 33
+    tot_ms = tot_emb = tot_balgc = 0
+    for i, q in enumerate(qs):
+        nb = int(sizes[int(q.array("labels")[mg.plan_order(q)[0]])])
+        step = max(1, nb // 64)
+        rec = None
+        while step <= nb:
+            try:
+                c, st = dg.count(q, stats=True, root_range=(0, nb), root_step=step,
+                                 max_elements=budget)
+                rec = {"q": i, "k": q.n, "bucket": nb, "step": step,
+                       "roots": (nb + step - 1) // step, "count": c, "device_ms": st["device_ms"],
+                       "elements": st["elements"], "balg_count_bytes": st["balg_count_bytes"]}
+                break
+            except L.MGError as e:
+                if e.code != L.MG_E_LIMIT:
+                    raise
+                step *= 4
+        if rec is None:
+            rec = {"q": i, "k": q.n, "bucket": nb, "over_budget": True}
+        else:
+            tot_ms += rec["device_ms"]
+            tot_emb += rec["count"]
+            tot_balgc += rec["balg_count_bytes"]
+        out["queries"].append(rec)
+    out["embeddings_per_s"] = tot_emb / (tot_ms / 1e3) if tot_ms else None
+    out["balg_count_gbs"] = tot_balgc / (tot_ms / 1e3) / 1e9 if tot_ms else None
+    out["device_ms"] = tot_ms
+    if oracle_check:
+        out["parity"] = c5_parity(g, dg, qs)
+    dg.free()
+    return out
+
+
+def c5_parity(g, dg, qs, n_check=2):
+    """Oracle counts of small strided samples of the first C5 queries (the
+    first stride from bucket/4 upward by factors of 4 whose GPU count is at
+    most 10^7), and whole emitted rows when the count is at most 10^5."""
+    import numpy as np
+
+    import matrixgraph_b200 as mg
+    import oracle as O
+    from matrixgraph_b200 import workloads as W
+    og = O.Graph.from_csr(g)
+    lab = g.array("labels")
+    sizes = np.bincount(lab, minlength=W.C5_LABELS)
+    checks = []
+    for i, q in enumerate(qs[:n_check]):
+        nb = int(sizes[int(q.array("labels")[mg.plan_order(q)[0]])])
+        step = max(1, nb // 4)
+        while step <= nb:
+            c = dg.count(q, root_range=(0, nb), root_step=step, max_elements=1 << 33)
+            if c <= 10 ** 7:
+                break
+            step *= 4
+        oq = O.query_from_csr(q)
+        t0 = time.perf_counter()
+        want = O.count(og, oq, threads=os.cpu_count() or 1, root_range=(0, nb),
+                       root_step=step)["count"]
+        rec = {"q": i, "step": step, "roots": (nb + step - 1) // step, "gpu": c,
+               "oracle": want, "equal": c == want,
+               "oracle_seconds": time.perf_counter() - t0}
+        if c <= 10 ** 5:
+            rows = dg.emit(q, root_range=(0, nb), root_step=step)
+            orows = O.emit(og, oq, cap=c, root_range=(0, nb), root_step=step)
+            rec["emit_rows"] = int(len(rows))
+            rec["emit_equal"] = bool(np.array_equal(rows, orows))
+        checks.append(rec)
+    return checks
+
+
 def heldout_summary():
     """Learned vs reference order on held-out 6-10-vertex queries, as recorded
     by `python -m matrixgraph_b200.workloads eval-order` (not re-measured)."""
@@ -516,6 +619,11 @@ def run_mine(args):
     if world == 1 and not args.no_batch and args.scale == 22 and not args.queries:
         batch = batched_workload(g, dg)
         _log("batched workload done")
+    c5 = None
+    if world == 1 and args.c5 > 0 and not args.queries:
+        dg.free()
+        c5 = c5_workload(args.c5)
+        _log("C5 workload done")
     gar = None
     if world == 1 and not args.no_gar:
         try:
@@ -538,6 +646,7 @@ def run_mine(args):
                          "seconds_per_step": e2e_s} if e2e_times else None),
                 "clocks": clocks, "gpu_launches": launches * args.steps,
                 "batched": batch, "learned_order_heldout": heldout_summary(), "gar_match": gar,
+                "c5": c5,
                 "graph": {"n": info["n"], "m_out": info["m_out"],
                           "device_bytes": info["device_bytes"], "max_degree": info["max_degree"],
                           "gen_seconds": gen_s}}

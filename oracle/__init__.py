@@ -64,8 +64,8 @@ _lib.orc_walk_labels.argtypes = [C.c_uint32, P32, P32, P32, C.c_uint32, P32, C.c
 _lib.orc_random_query_shape.argtypes = [C.c_uint32, C.c_double, C.c_uint64, P32]
 _libc = C.CDLL(None)
 _libc.free.argtypes = [C.c_void_p]
-_lib.orc_emit.argtypes = [C.c_void_p, C.POINTER(OrcQuery), P32, C.c_uint32, P32, C.c_uint64,
-                          C.POINTER(C.c_uint64)]
+_lib.orc_emit.argtypes = [C.c_void_p, C.POINTER(OrcQuery), P32, C.c_uint32, C.c_uint64,
+                          C.c_uint64, C.c_uint64, P32, C.c_uint64, C.POINTER(C.c_uint64)]
 _lib.orc_bucket_size.restype = C.c_uint32
 _lib.orc_bucket_size.argtypes = [C.c_void_p, C.POINTER(OrcQuery), P32]
 
@@ -156,13 +156,18 @@ def count(g: Graph, q: OrcQuery, order=None, filters=3, threads=1, root_range=No
             "balg_count": r.balg_count, "order": order}
 
 
-def emit(g: Graph, q: OrcQuery, order=None, filters=3, cap=None) -> np.ndarray:
+def emit(g: Graph, q: OrcQuery, order=None, filters=3, cap=None, root_range=None,
+         root_step=1) -> np.ndarray:
+    """Sorted match rows over the level-0 positions begin, begin + root_step, ...
+    below end (root_range None: the whole bucket)."""
     order = reference_order(q) if order is None else list(order)
+    rb, re_ = (0, 2 ** 64 - 1) if root_range is None else root_range
     if cap is None:
-        cap = count(g, q, order, filters)["count"]
+        cap = count(g, q, order, filters, root_range=(rb, re_), root_step=root_step)["count"]
     rows = np.zeros((max(cap, 1), q.k), dtype=np.uint32)
     n = C.c_uint64()
-    rc = _lib.orc_emit(g.h, C.byref(q), _p(_u32(order)), filters, _p(rows), cap, C.byref(n))
+    rc = _lib.orc_emit(g.h, C.byref(q), _p(_u32(order)), filters, rb, re_, max(1, root_step),
+                       _p(rows), cap, C.byref(n))
     if rc:
         raise RuntimeError(f"oracle emit failed: {rc}")
     return rows[:min(cap, n.value)]

@@ -759,11 +759,14 @@ static int cmp_rows(const void* a, const void* b) {
   return 0;
 }
 
-/* All matches as rows in query-vertex order, lexicographically sorted. */
+/* All matches as rows in query-vertex order, lexicographically sorted, over
+ * the level-0 candidates at bucket positions root_begin, root_begin +
+ * root_step, ... below root_end. */
 int orc_emit(const orc_graph* g, const orc_query* q, const uint32_t* order, uint32_t filters,
-             uint32_t* rows, uint64_t cap, uint64_t* n_rows) {
+             uint64_t root_begin, uint64_t root_end, uint64_t root_step, uint32_t* rows,
+             uint64_t cap, uint64_t* n_rows) {
   orc_result res;
-  int rc = run(g, q, order, filters, 1, 0, UINT64_MAX, 1, rows, cap, &res, n_rows);
+  int rc = run(g, q, order, filters, 1, root_begin, root_end, root_step, rows, cap, &res, n_rows);
   if (rc) return rc;
   g_row_k = q->k;
   qsort(rows, *n_rows < cap ? *n_rows : cap, (size_t)q->k * 4, cmp_rows);
