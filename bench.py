@@ -370,17 +370,23 @@ def gar_workload(reps=3):
     return out
 
 
-def c5_workload(n_queries, oracle_check=True):
+C5_GOLDEN = os.path.join(ROOT, "tests", "golden", "c5_samples.json")
+
+
+def c5_workload(n_queries):
     """Configuration C5: R-MAT scale 26 (67,108,864 vertices, ~2.1e9 directed
     entries) with 64 Zipf(1.2) labels, queries of 6-8 vertices (4-clique or
     chorded 5-cycle plus a pendant path).  Their reference-order counts run to
-    10^13-10^15 embeddings, so each query is counted over a strided sample of
-    its level-0 candidates: positions 0, s, 2s, ... with the smallest s (from
-    bucket/64 upward by factors of 4) whose enumeration needs at most 2^33
-    candidate elements (element counts are exact, so the sample does not
-    depend on timing).  The oracle then counts a smaller sample of two queries
-    (the first stride whose GPU count is at most 10^7) for parity, and the
-    emitted rows of a sample with at most 10^5 matches are compared whole."""
+    10^13-10^15 embeddings, so each query is counted over a systematic sample
+    of its level-0 candidates: positions s/2, s/2 + s, ... with the smallest
+    stride s (from bucket/256 upward by factors of 4) whose enumeration needs
+    at most 2^33 candidate elements (element counts are exact, so the sample
+    does not depend on timing).  Parity: the GPU counts the fixed low-degree
+    samples of tests/golden/c5_samples.json, whose counts (and sorted rows,
+    through their SHA-256) the oracle computed on the CPU
+    (tests/golden/make_c5_golden.py)."""
+    import hashlib
+
     import numpy as np
 
     import matrixgraph_b200 as mg
@@ -392,27 +398,28 @@ def c5_workload(n_queries, oracle_check=True):
     dg = mg.DeviceGraph(g, 0)
     upload_s = time.perf_counter() - t0 - gen_s
     info = dg.info
+    _log(f"C5 graph generated ({gen_s:.0f} s) and uploaded ({upload_s:.0f} s)")
     qs = W.c5_queries(g, n_queries)
-    lab = g.array("labels")
-    sizes = np.bincount(lab, minlength=W.C5_LABELS)
+    sizes = np.bincount(g.array("labels"), minlength=W.C5_LABELS)
     out = {"workload": f"R-MAT scale 26 ({g.n:,} vertices, {g.m_out:,} directed entries), 64 "
                        f"Zipf(1.2) labels; first {n_queries} C5 queries (k 6-8), reference "
-                       "order, count mode over strided root samples",
+                       "order, count mode over systematic root samples",
            "gen_seconds": gen_s, "upload_seconds": upload_s,
            "device_bytes": info["device_bytes"], "queries": []}
     budget = 1 << 33
     tot_ms = tot_emb = tot_balgc = 0
     for i, q in enumerate(qs):
         nb = int(sizes[int(q.array("labels")[mg.plan_order(q)[0]])])
-        step = max(1, nb // 64)
+        step = max(1, nb // 256)
         rec = None
         while step <= nb:
             try:
-                c, st = dg.count(q, stats=True, root_range=(0, nb), root_step=step,
+                c, st = dg.count(q, stats=True, root_range=(step // 2, nb), root_step=step,
                                  max_elements=budget)
-                rec = {"q": i, "k": q.n, "bucket": nb, "step": step,
-                       "roots": (nb + step - 1) // step, "count": c, "device_ms": st["device_ms"],
-                       "elements": st["elements"], "balg_count_bytes": st["balg_count_bytes"]}
+                rec = {"q": i, "k": q.n, "bucket": nb, "begin": step // 2, "step": step,
+                       "roots": (nb - step // 2 + step - 1) // step, "count": c,
+                       "device_ms": st["device_ms"], "elements": st["elements"],
+                       "balg_count_bytes": st["balg_count_bytes"]}
                 break
             except L.MGError as e:
                 if e.code != L.MG_E_LIMIT:
@@ -428,47 +435,34 @@ def c5_workload(n_queries, oracle_check=True):
     out["embeddings_per_s"] = tot_emb / (tot_ms / 1e3) if tot_ms else None
     out["balg_count_gbs"] = tot_balgc / (tot_ms / 1e3) / 1e9 if tot_ms else None
     out["device_ms"] = tot_ms
-    if oracle_check:
-        out["parity"] = c5_parity(g, dg, qs)
+    _log("C5 samples counted")
+    # parity against the committed oracle counts of fixed low-degree samples
+    parity = []
+    try:
+        with open(C5_GOLDEN) as f:
+            gold = json.load(f)
+    except OSError:
+        gold = {"queries": []}
+    for rec in gold["queries"]:
+        if "count" not in rec:
+            continue
+        q = mg.query_walk(g, (rec["k"], [tuple(e) for e in rec["edges"]]),
+                          seed=W.C5_FIRST_SEED + rec["q"])
+        same_query = q.array("labels").tolist() == rec["labels"]
+        c, st = dg.count(q, stats=True, root_range=(rec["begin"], rec["end"]))
+        p = {"q": rec["q"], "roots": rec["end"] - rec["begin"], "oracle": rec["count"],
+             "gpu": c, "equal": same_query and c == rec["count"] and
+             st["level_rows"] == rec["level_rows"]}
+        if "rows_sha256" in rec:
+            rows = dg.emit(q, root_range=(rec["begin"], rec["end"]))
+            h = hashlib.sha256(np.ascontiguousarray(rows, dtype="<u4").tobytes()).hexdigest()
+            p["rows_equal"] = h == rec["rows_sha256"]
+        parity.append(p)
+    out["parity"] = {"source": "tests/golden/c5_samples.json", "samples": parity,
+                     "all_equal": bool(parity) and all(p["equal"] and p.get("rows_equal", True)
+                                                       for p in parity)}
     dg.free()
     return out
-
-
-def c5_parity(g, dg, qs, n_check=2):
-    """Oracle counts of small strided samples of the first C5 queries (the
-    first stride from bucket/4 upward by factors of 4 whose GPU count is at
-    most 10^7), and whole emitted rows when the count is at most 10^5."""
-    import numpy as np
-
-    import matrixgraph_b200 as mg
-    import oracle as O
-    from matrixgraph_b200 import workloads as W
-    og = O.Graph.from_csr(g)
-    lab = g.array("labels")
-    sizes = np.bincount(lab, minlength=W.C5_LABELS)
-    checks = []
-    for i, q in enumerate(qs[:n_check]):
-        nb = int(sizes[int(q.array("labels")[mg.plan_order(q)[0]])])
-        step = max(1, nb // 4)
-        while step <= nb:
-            c = dg.count(q, root_range=(0, nb), root_step=step, max_elements=1 << 33)
-            if c <= 10 ** 7:
-                break
-            step *= 4
-        oq = O.query_from_csr(q)
-        t0 = time.perf_counter()
-        want = O.count(og, oq, threads=os.cpu_count() or 1, root_range=(0, nb),
-                       root_step=step)["count"]
-        rec = {"q": i, "step": step, "roots": (nb + step - 1) // step, "gpu": c,
-               "oracle": want, "equal": c == want,
-               "oracle_seconds": time.perf_counter() - t0}
-        if c <= 10 ** 5:
-            rows = dg.emit(q, root_range=(0, nb), root_step=step)
-            orows = O.emit(og, oq, cap=c, root_range=(0, nb), root_step=step)
-            rec["emit_rows"] = int(len(rows))
-            rec["emit_equal"] = bool(np.array_equal(rows, orows))
-        checks.append(rec)
-    return checks
 
 
 def heldout_summary():

@@ -52,7 +52,7 @@ typedef struct orc_graph {
   uint32_t* label_values; /* compact -> raw, ascending */
   uint32_t* globalid;
   uint32_t* adj[2];       /* per direction: lists ordered by (label, id) */
-  uint64_t* loff[2];      /* n*L + 1 slice starts */
+  uint32_t* loff[2];      /* n*L + 1 slice starts (the format's uint32 offsets) */
   uint32_t* deg[2];
   uint32_t* nlb[2];       /* n*W */
   uint32_t* bucket_off;   /* L + 1 */
@@ -220,7 +220,7 @@ static void slice_vertex(void* p, uint32_t v) {
   qsort(c->adj + s, e - s, 4, cmp_lab_id);
   uint64_t q = s;
   for (uint32_t l = 0; l < L; ++l) {
-    g->loff[d][(uint64_t)v * L + l] = q;
+    g->loff[d][(uint64_t)v * L + l] = (uint32_t)q;
     while (q < e && g->label[c->adj[q]] == l) ++q;
     if (g->loff[d][(uint64_t)v * L + l] < q) g->nlb[d][(uint64_t)v * W + l / 32] |= 1u << (l % 32);
   }
@@ -302,13 +302,13 @@ orc_graph* orc_graph_from_arrays(uint32_t n, uint32_t max_vid, const uint32_t* g
       break;
     }
     uint32_t L = g->L, W = g->W;
-    g->loff[d] = (uint64_t*)malloc(((size_t)n * L + 1) * 8);
+    g->loff[d] = (uint32_t*)malloc(((size_t)n * L + 1) * 4);
     g->deg[d] = (uint32_t*)malloc((size_t)n * 4);
     g->nlb[d] = (uint32_t*)calloc((size_t)n * W, 4);
     g_sort_labels = g->label;
     slice_ctx sc = {g, d, off[d], adj[d]};
     par_for(n, slice_vertex, &sc);
-    g->loff[d][(uint64_t)n * L] = off[d][n];
+    g->loff[d][(uint64_t)n * L] = (uint32_t)off[d][n];
     g->adj[d] = adj[d];
     free(off[d]);
   }
@@ -590,7 +590,7 @@ static int passes(const thread_ctx* T, uint32_t i, uint32_t x) {
     if (T->m[j] == x) return 0;
   for (uint32_t c = 0; c < P->nc[i]; ++c) {
     uint32_t y = T->m[P->cpos[i][c]], d = P->cdir[i][c];
-    const uint64_t* lo = g->loff[d] + (uint64_t)y * g->L + P->label[i];
+    const uint32_t* lo = g->loff[d] + (uint64_t)y * g->L + P->label[i];
     if (!contains(g->adj[d], lo[0], lo[1], x)) return 0;
   }
   if (P->self[i] && !g->self[x]) return 0;
@@ -649,7 +649,7 @@ static void extend(thread_ctx* T, uint32_t i) {
     s = e = 0;
     for (uint32_t c = 0; c < P->nc[i]; ++c) {
       uint32_t y = T->m[P->cpos[i][c]], d = P->cdir[i][c];
-      const uint64_t* lo = g->loff[d] + (uint64_t)y * g->L + lab;
+      const uint32_t* lo = g->loff[d] + (uint64_t)y * g->L + lab;
       uint64_t len = lo[1] - lo[0];
       charge += 8 + 4 * len;
       if (len < best) {
