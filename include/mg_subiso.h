@@ -332,6 +332,17 @@ int  mg_order_model_predict(void* model, void* dgraph, const mg_csr_view* const*
 int  mg_order_model_features(void* dgraph, const mg_csr_view* q, float* x, float* e,
                              uint32_t* adj);
 
+/* Self-test of the bounded device waits (no counterpart in the reference;
+ * the reference has no device-side wait).  The batch lane pipeline's
+ * work/scan kernel waits, tile by tile, for the sums of earlier tiles; every
+ * such wait gives up after a fixed number of polls and the call then returns
+ * MG_E_TIMEOUT instead of spinning.  This entry point runs that kernel once
+ * with the first tile never handed out, so the wait for it must run out:
+ * *status receives MG_E_TIMEOUT when the bound worked (MG_OK otherwise).
+ * `q` needs a second vertex joined to its first; spin_limit >= 1 polls.    */
+int  mg_selftest_wait_timeout(void* dgraph, const mg_csr_view* q, uint32_t spin_limit,
+                              int* status);
+
 /* Exact count that allocates nothing.  No counterpart in the reference.
  *
  * For callers that cannot allocate device memory when they ask for a count:

@@ -1906,6 +1906,75 @@ static int subiso_batch_lanes(DevGraph* dg, std::vector<PlanDev>& plans, const m
   return MG_OK;
 }
 
+// Self-test of the bounded device wait: one work/scan launch of a lane at
+// level 1 over 2 * WS_ROWS rows of the first query vertex's bucket, with the
+// counter that hands out tiles already past tile 0, so the block of tile 1
+// waits for a predecessor nobody publishes.  The wait gives up after
+// `spin_limit` polls and the launch ends with ERR_TIMEOUT in its error word.
+static int selftest_wait(DevGraph* dg, const mg_csr_view* q, uint32_t spin_limit,
+                         uint64_t* err_bits) {
+  PlanDev P;
+  mg_opts o;
+  mg_opts_default(&o);
+  int rc = prepare(dg, q, o, &P);
+  if (rc) return rc;
+  if (P.k < 2 || P.ncons[1] == 0)
+    return set_error(MG_E_ARG, "self-test query needs a second vertex joined to the first");
+  if ((rc = ensure_lanes(dg, 1, kLaneCap, std::max<uint32_t>(P.k, 2)))) return rc;
+  LaneSet* ls = dg->lanes;
+  Lane& L = ls->lanes[0];
+  if (ls->plans_cap < 1) {
+    if ((rc = lane_alloc(ls, (void**)&ls->plans, sizeof(PlanDev)))) return rc;
+    ls->plans_cap = 1;
+  }
+  cudaStream_t st = L.st;
+  const uint64_t rows = 2 * WS_ROWS;
+  std::vector<unsigned long long> ctr(C_NUM, 0);
+  ctr[C_LOUT + 0] = rows;  // level-1 table holds `rows` rows
+  ctr[C_LSCAN + 1] = 1;    // tile 0 of level 1 is never handed out
+  MG_CK(cudaMemcpyAsync(ls->plans, &P, sizeof(PlanDev), cudaMemcpyHostToDevice, st));
+  MG_CK(cudaMemcpyAsync(L.ctr, ctr.data(), C_NUM * 8, cudaMemcpyHostToDevice, st));
+  // every row holds the first vertex of the bucket of position 0
+  const uint32_t b0 = dg->h_bucket_off[P.label[0]];
+  std::vector<uint32_t> col(rows, 0);
+  MG_CK(cudaMemcpyAsync(col.data(), dg->g.bucket_vid + b0, 4, cudaMemcpyDeviceToHost, st));
+  MG_CK(cudaStreamSynchronize(st));
+  for (uint64_t r = 1; r < rows; ++r) col[r] = col[0];
+  MG_CK(cudaMemcpyAsync(L.col[1][0], col.data(), rows * 4, cudaMemcpyHostToDevice, st));
+  StepArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.g = dg->g;
+  a.plans = ls->plans;
+  a.ctr = L.ctr;
+  a.counts = L.counts;
+  a.lvl_rows = L.lvl;
+  a.q_elems = L.qel;
+  a.level = 1;
+  a.in.col[0] = L.col[1][0];
+  a.work = L.work[1];
+  a.woff = L.woff[1];
+  a.dstart = L.dstart[1];
+  a.dci = L.dci[1];
+  a.lane = 1;
+  a.cap_rows = ls->cap;
+  a.seg_cap = ls->seg_cap;
+  a.scan_status = L.status;
+  a.spin_limit = spin_limit;
+  a.root_step = 1;
+  if (++L.epoch > kEpochMax) {
+    MG_CK(cudaMemsetAsync(L.status, 0, (ls->cap / WS_ROWS + 2) * 8, st));
+    L.epoch = 1;
+  }
+  k_work_scan<<<2, 256, 0, st>>>(a, L.epoch);
+  MG_CK(cudaGetLastError());
+  unsigned long long err = 0;
+  MG_CK(cudaMemcpyAsync(&err, L.ctr + C_ERR, 8, cudaMemcpyDeviceToHost, st));
+  MG_CK(cudaMemsetAsync(L.ctr, 0, C_NUM * 8, st));
+  MG_CK(cudaStreamSynchronize(st));
+  *err_bits = err;
+  return MG_OK;
+}
+
 int subiso_batch(DevGraph* dg, const mg_csr_view* const* qs, uint32_t nq, const mg_opts* opts,
                  uint64_t* counts, mg_stats* st, const uint32_t* orders = nullptr,
                  uint64_t* level_rows = nullptr) {
@@ -2062,6 +2131,17 @@ int mg_subiso_batch_count_orders(void* dgraph, const mg_csr_view* const* qs, uin
   } catch (const std::bad_alloc&) {
     return mg::set_error(MG_E_OOM, "host allocation failed");
   }
+}
+
+int mg_selftest_wait_timeout(void* dgraph, const mg_csr_view* q, uint32_t spin_limit,
+                             int* status) {
+  MG_ENTRY(dgraph);
+  if (!q || !status || spin_limit == 0) return mg::set_error(MG_E_ARG, "bad argument");
+  uint64_t err = 0;
+  int rc = mg::selftest_wait(dg, q, spin_limit, &err);
+  if (rc) return rc;
+  *status = (err & mg::ERR_TIMEOUT) ? MG_E_TIMEOUT : MG_OK;
+  return MG_OK;
 }
 
 }  // extern "C"

@@ -10,10 +10,13 @@
 //
 //   ref_gar_match IN OUT
 // IN (little-endian): int32 n_vertices, n_edges, p_nodes, p_edges,
-// row_capacity, match_capacity; then uint32 v_id[n_vertices], int32
-// v_label[n_vertices], uint32 e_src[n_edges], e_dst[n_edges], e_id[n_edges],
-// int32 e_label[n_edges], p_node_label[p_nodes], p_edge_src[p_edges],
-// p_edge_dst[p_edges], p_edge_label[p_edges].
+// row_capacity, match_capacity, has_v_id, has_e_label, has_p_edge_label;
+// then uint32 v_id[n_vertices], int32 v_label[n_vertices], uint32
+// e_src[n_edges], e_dst[n_edges], e_id[n_edges], int32 e_label[n_edges],
+// p_node_label[p_nodes], p_edge_src[p_edges], p_edge_dst[p_edges],
+// p_edge_label[p_edges].  An array whose has_ flag is 0 is passed to the
+// reference as a null pointer (its contents in the file are ignored), as
+// the reference treats absent ids and edge labels.
 // OUT: int32 status, num_conditions, row_size, match_size; then row_size
 // entries each of uint32 pivot, int32 cond_j, pos, offset, count; then uint32
 // matched_v_ids[match_size].  The reference's own log goes to stdout.
@@ -38,8 +41,8 @@ int main(int argc, char** argv) {
   }
   FILE* in = std::fopen(argv[1], "rb");
   if (!in) return 2;
-  int32_t h[6];
-  if (std::fread(h, 4, 6, in) != 6) return 2;
+  int32_t h[9];
+  if (std::fread(h, 4, 9, in) != 9) return 2;
   const int nv = h[0], ne = h[1], pn = h[2], pe = h[3], row_cap = h[4], match_cap = h[5];
   std::vector<uint32_t> v_id, e_src, e_dst, e_id;
   std::vector<int32_t> v_label, e_label, p_label, p_src, p_dst, p_elabel;
@@ -49,9 +52,10 @@ int main(int argc, char** argv) {
             read_vec(in, p_elabel, pe);
   std::fclose(in);
   if (!ok) return 2;
-  K::GARGraphArrays g{v_id.data(), v_label.data(), nv, e_src.data(), e_dst.data(),
-                      e_id.data(), e_label.data(), ne};
-  K::GARPatternArrays p{p_label.data(), pn, p_src.data(), p_dst.data(), p_elabel.data(), pe};
+  K::GARGraphArrays g{h[6] ? v_id.data() : nullptr, v_label.data(), nv, e_src.data(),
+                      e_dst.data(), e_id.data(), h[7] ? e_label.data() : nullptr, ne};
+  K::GARPatternArrays p{p_label.data(), pn, p_src.data(), p_dst.data(),
+                        h[8] ? p_elabel.data() : nullptr, pe};
   int num_conditions = 0, row_size = 0, match_size = 0;
   std::vector<uint32_t> pivot(size_t(row_cap > 0 ? row_cap : 1)),
       ids(size_t(match_cap > 0 ? match_cap : 1));

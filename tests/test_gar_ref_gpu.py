@@ -12,7 +12,9 @@ core/task/gpu_task/kernel/kernel_gar_match.cu where it lies
 
 Inputs are valid by construction (every edge endpoint below n_vertices,
 pattern indices below n_nodes), the cases are small, and every capacity is
-set so that the reference's own guards keep all writes in bounds."""
+set so that the reference's own guards keep all writes in bounds.  Every
+array is present: the reference copies each input array to the device
+unconditionally, so a missing array is not an input it defines."""
 import os
 import struct
 import subprocess
@@ -37,17 +39,15 @@ def run_reference(g, p, row_cap, match_cap):
     """The reference's GARMatchKernelWrapper::GARMatch on (g, p); returns
     (status, num_conditions, rows[(pivot, cond_j, pos, offset, count)], ids)."""
     n, m, k, pe = g.n_vertices, len(g.e_src), p.n_nodes, len(p.edge_src)
-    v_id = g.v_id if g.v_id is not None else list(range(n))
-    e_label = g.e_label if g.e_label is not None else [0] * m
-    p_elabel = p.edge_label if p.edge_label is not None else [0] * pe
+    assert g.v_id is not None and g.e_label is not None and p.edge_label is not None
     with tempfile.TemporaryDirectory() as d:
         fin, fout = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
         with open(fin, "wb") as f:
-            f.write(struct.pack("<6i", n, m, k, pe, row_cap, match_cap))
-            for arr, dt in ((v_id, "<u4"), (g.v_label, "<i4"), (g.e_src, "<u4"),
-                            (g.e_dst, "<u4"), (list(range(m)), "<u4"), (e_label, "<i4"),
+            f.write(struct.pack("<9i", n, m, k, pe, row_cap, match_cap, 1, 1, 1))
+            for arr, dt in ((g.v_id, "<u4"), (g.v_label, "<i4"), (g.e_src, "<u4"),
+                            (g.e_dst, "<u4"), (list(range(m)), "<u4"), (g.e_label, "<i4"),
                             (p.node_label, "<i4"), (p.edge_src, "<i4"), (p.edge_dst, "<i4"),
-                            (p_elabel, "<i4")):
+                            (p.edge_label, "<i4")):
                 f.write(np.asarray(arr, dtype=dt).tobytes())
         r = subprocess.run([EXE, fin, fout], capture_output=True, text=True, timeout=300)
         assert r.returncode == 0, r.stderr[-2000:]
@@ -91,10 +91,10 @@ def test_reference_output_pins_the_restatement_and_the_engine():
     for seed in range(40):
         rng = np.random.default_rng(900 + seed)
         n = int(rng.integers(8, 40))
-        g = random_graph(rng, n, int(rng.integers(n, 5 * n)), v_labels=3, e_labels=2,
-                         with_ids=seed % 3 != 0, with_elabels=seed % 4 != 0)
+        g = random_graph(rng, n, int(rng.integers(n, 5 * n)), v_labels=3,
+                         e_labels=1 + seed % 2)
         p = random_pattern(rng, int(rng.integers(2, 5)), int(rng.integers(0, 3)), v_labels=3,
-                           e_labels=2, with_elabels=seed % 5 != 0)
+                           e_labels=1 + seed % 2)
         rcap, mcap = 1000, 4000
         status, nc, rows, ids = run_reference(g, p, rcap, mcap)
         assert status == 0

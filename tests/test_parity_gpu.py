@@ -421,3 +421,18 @@ def test_batch_lane_pipeline_variants(c1):
     ref = [dg.count(x, no_tail=1) for x in tq]
     assert dg.batch_count(tq).tolist() == ref
     assert dg.batch_count(tq, no_tail=1).tolist() == ref
+
+
+def test_bounded_device_wait_times_out_and_context_stays_usable(c1):
+    """The lane pipeline's look-back wait gives up after its poll limit: a
+    work/scan launch whose first tile is never handed out reports
+    MG_E_TIMEOUT, and the graph handle keeps counting correctly after it."""
+    import ctypes as C
+    g, q, dg = c1
+    for limit in (1, 64, 4096):
+        status = C.c_int(12345)
+        L.check(L.lib.mg_selftest_wait_timeout(dg.handle, C.byref(q.view), limit,
+                                               C.byref(status)))
+        assert status.value == L.MG_E_TIMEOUT, limit
+    qs = [mg.query_random(g, 3 + i % 4, 0.3, seed=7000 + i) for i in range(16)]
+    assert dg.batch_count(qs).tolist() == [dg.count(x) for x in qs]
