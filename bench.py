@@ -302,10 +302,25 @@ def same_work(dg, qs, names, cpu_rows, device, e2e_graph):
             "speedup_e2e": cpu_s / e2e_s if e2e_s > 0 else None}
 
 
-def batched_workload(g, dg):
-    """The committed 4,096-query batch on the same resident graph: the plain
-    per-query heuristic-order form against one batched call with learned
-    orders (planning included), wall clock, counts checked per query."""
+def c3_oracle_sample(g, og, every=64, max_elements=10 ** 7):
+    """Oracle counts of a systematic sample of the 4,096-query batch: every
+    `every`-th query among those whose reference order expands at most
+    `max_elements` candidates.  Returns {index: count}."""
+    import oracle as O
+    from matrixgraph_b200 import workloads as W
+    qs, rec = W.batch_queries(g)
+    picked = [i for i in range(0, len(qs), every) if rec["elements"][i] <= max_elements]
+    threads = os.cpu_count() or 1
+    return {i: O.count(og, O.query_from_csr(qs[i]), threads=threads)["count"] for i in picked}
+
+
+def batched_workload(g, dg, oracle_counts=None):
+    """The 4,096-query batch on the same resident graph: the per-query
+    heuristic-order form (one call per query) against batched calls — the
+    lane pipeline (every query a fixed launch sequence with device-side sizes
+    on 8 concurrent streams, one host wait per batch) with the reference and
+    with learned orders (planning included) — wall clock.  Every form's counts
+    equal the per-query counts, and a systematic sample equals the oracle."""
     from matrixgraph_b200 import workloads as W
     from matrixgraph_b200.order_model import OrderModel
     qs, rec = W.batch_queries(g)
@@ -313,20 +328,28 @@ def batched_workload(g, dg):
     out = {"workload": f"{len(qs)} random connected queries (k 3-8, p_extra 0.3, random-walk "
                        "labels; seeds kept when the reference order needs <= 2^28 elements, "
                        "matrixgraph_b200/data/batch_seeds.json), count mode"}
+    ref_counts = None
     for name, fn in (("per_query_reference", lambda: [dg.count(q) for q in qs]),
                      ("batch_reference", lambda: dg.batch_count(qs).tolist()),
                      ("batch_learned", lambda: dg.batch_count(qs, order="learned",
                                                               model=model).tolist())):
         fn()  # warm-up
         t0 = time.perf_counter()
-        counts = fn()
+        counts = [int(c) for c in fn()]
         wall = time.perf_counter() - t0
-        assert [int(c) for c in counts] == rec["counts"], name
+        if ref_counts is None:
+            ref_counts = counts
+        assert counts == ref_counts, name
         out[name] = {"seconds": wall, "queries_per_s": len(qs) / wall}
         _log(f"batched {name}: {wall:.2f} s")
     base = out["per_query_reference"]["seconds"]
     for name in ("batch_reference", "batch_learned"):
         out[name]["speedup_vs_per_query_reference"] = base / out[name]["seconds"]
+    out["counts_equal_recorded"] = ref_counts == rec["counts"]
+    if oracle_counts:
+        out["oracle_sample"] = {"queries": sorted(oracle_counts),
+                                "equal": all(ref_counts[i] == c for i, c in oracle_counts.items())}
+        assert out["oracle_sample"]["equal"], "batch counts differ from the oracle"
     model.free()
     return out
 
@@ -449,12 +472,14 @@ def c5_workload(n_queries):
         q = mg.query_walk(g, (rec["k"], [tuple(e) for e in rec["edges"]]),
                           seed=W.C5_FIRST_SEED + rec["q"])
         same_query = q.array("labels").tolist() == rec["labels"]
-        c, st = dg.count(q, stats=True, root_range=(rec["begin"], rec["end"]))
-        p = {"q": rec["q"], "roots": rec["end"] - rec["begin"], "oracle": rec["count"],
+        rr, rs = (rec["begin"], rec["end"]), rec.get("step", 1)
+        c, st = dg.count(q, stats=True, root_range=rr, root_step=rs)
+        p = {"q": rec["q"], "roots": (rec["end"] - rec["begin"] + rs - 1) // rs,
+             "oracle": rec["count"],
              "gpu": c, "equal": same_query and c == rec["count"] and
              st["level_rows"] == rec["level_rows"]}
         if "rows_sha256" in rec:
-            rows = dg.emit(q, root_range=(rec["begin"], rec["end"]))
+            rows = dg.emit(q, root_range=rr, root_step=rs)
             h = hashlib.sha256(np.ascontiguousarray(rows, dtype="<u4").tobytes()).hexdigest()
             p["rows_equal"] = h == rec["rows_sha256"]
         parity.append(p)
@@ -465,18 +490,76 @@ def c5_workload(n_queries):
     return out
 
 
-def heldout_summary():
-    """Learned vs reference order on held-out 6-10-vertex queries, as recorded
-    by `python -m matrixgraph_b200.workloads eval-order` (not re-measured)."""
-    path = os.path.join(ROOT, "matrixgraph_b200", "data", "order_eval.json")
-    try:
-        with open(path) as f:
-            sm = json.load(f)["summary"]
-    except Exception:
-        return None
-    keep = ("n", "median_speedup_device", "geomean_speedup_device", "median_regret",
-            "total_ms_ref", "total_ms_learned")
-    return {"source": "matrixgraph_b200/data/order_eval.json", **{k: sm.get(k) for k in keep}}
+def heldout_eval(dg, g, n=512, budget=1 << 28):
+    """Learned vs reference order on held-out queries (configuration C4):
+    seeds 200000 .. 200000+n-1 taken in order — the selection depends on
+    neither order — random connected, k uniform 6-10, walk labels, on the
+    resident scale-22 graph.  The orders of the whole set are planned in one
+    call each (the learned one through one inference launch; its time is the
+    planning cost), and every query is counted under both orders with the
+    same element budget.  A query past the budget under an order is censored
+    there: a censored reference against a finished learned order counts as a
+    win, the reverse as a loss, and queries censored under both are left out
+    of the medians.  Counts under both orders must be equal."""
+    import numpy as np
+
+    from matrixgraph_b200 import _lib as L
+    from matrixgraph_b200 import workloads as W
+    from matrixgraph_b200.order_model import OrderModel
+    model = OrderModel.load(W.MODEL_DIR)
+    qs = [W.learned_query(g, W.EVAL_FIRST_SEED + i) for i in range(n)]
+    ref_orders = dg.plan_orders(qs, order="reference")
+    t0 = time.perf_counter()
+    learned_orders = dg.plan_orders(qs, order="learned", model=model)
+    plan_s = time.perf_counter() - t0
+    model.free()
+    res = []
+    for q, ro, lo in zip(qs, ref_orders, learned_orders):
+        r = {}
+        for name, od in (("ref", ro), ("learned", lo)):
+            try:
+                c, st = dg.count(q, stats=True, given_order=od, max_elements=budget)
+                r[name] = (c, st["device_ms"], st["elements"])
+            except L.MGError as e:
+                if e.code != L.MG_E_LIMIT:
+                    raise
+                r[name] = None
+        if r["ref"] and r["learned"]:
+            assert r["ref"][0] == r["learned"][0], "counts differ between orders"
+        res.append(r)
+    plan_ms = 1e3 * plan_s / n
+    sp, sp_plan, el, sp_both = [], [], [], []
+    both = ref_only = learned_only = neither = 0
+    for r in res:
+        a, b = r["ref"], r["learned"]
+        if a and b:
+            both += 1
+            sp.append(a[1] / b[1])
+            sp_both.append(a[1] / b[1])
+            sp_plan.append(a[1] / (b[1] + plan_ms))
+            el.append(a[2] / max(1, b[2]))
+        elif b:
+            learned_only += 1
+            sp.append(float("inf"))
+            sp_plan.append(float("inf"))
+        elif a:
+            ref_only += 1
+            sp.append(0.0)
+            sp_plan.append(0.0)
+        else:
+            neither += 1
+    med = float(np.median(sp)) if sp else None
+    return {"workload": f"{n} held-out random connected queries (seeds 200000..{200000 + n - 1}, "
+                        "k 6-10, p_extra 0.3, walk labels) on the R-MAT scale-22 graph; budget "
+                        f"{budget} candidate elements per count",
+            "model": "matrixgraph_b200/data/order_model", "n": n,
+            "finished_both": both, "finished_learned_only": learned_only,
+            "finished_reference_only": ref_only, "finished_neither": neither,
+            "median_speedup_device": med,
+            "median_speedup_with_planning": float(np.median(sp_plan)) if sp_plan else None,
+            "median_speedup_device_both_finished": float(np.median(sp_both)) if sp_both else None,
+            "median_element_ratio_both_finished": float(np.median(el)) if el else None,
+            "planning_ms_per_query": plan_ms}
 
 
 def run_mine(args):
@@ -491,13 +574,15 @@ def run_mine(args):
     gen_s = time.perf_counter() - t0
     _log("workload generated")
     # The oracle runs before this process initialises CUDA.
-    cpu, cpu_rows = None, None
+    cpu, cpu_rows, c3_oracle = None, None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle as O
         threads = os.cpu_count() or 1
         og = O.Graph.from_csr(g)
         oqs = [O.query_from_csr(q) for q in qs]
         cpu_rows = oracle_sample(og, oqs, names, threads)
+        if not args.no_batch and args.scale == 22 and not args.queries:
+            c3_oracle = c3_oracle_sample(g, og)
         del og
         c, s = sum(r[4] for r in cpu_rows), sum(r[5] for r in cpu_rows)
         cpu = {"value": c / s if s > 0 else 0.0, "unit": "embeddings/s", "cores": threads,
@@ -611,8 +696,12 @@ def run_mine(args):
                 "step_rate_gbs": balgc / (ms_step / 1e3) / 1e9}
     batch = None
     if world == 1 and not args.no_batch and args.scale == 22 and not args.queries:
-        batch = batched_workload(g, dg)
+        batch = batched_workload(g, dg, c3_oracle)
         _log("batched workload done")
+    heldout = None
+    if world == 1 and not args.no_batch and args.scale == 22 and not args.queries:
+        heldout = heldout_eval(dg, g)
+        _log("held-out order evaluation done")
     c5 = None
     if world == 1 and args.c5 > 0 and not args.queries:
         dg.free()
@@ -639,7 +728,7 @@ def run_mine(args):
                          "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                          "seconds_per_step": e2e_s} if e2e_times else None),
                 "clocks": clocks, "gpu_launches": launches * args.steps,
-                "batched": batch, "learned_order_heldout": heldout_summary(), "gar_match": gar,
+                "batched": batch, "learned_order_heldout": heldout, "gar_match": gar,
                 "c5": c5,
                 "graph": {"n": info["n"], "m_out": info["m_out"],
                           "device_bytes": info["device_bytes"], "max_degree": info["max_degree"],

@@ -247,6 +247,12 @@ int  mg_query_from_edges(uint32_t k, const uint32_t* eu, const uint32_t* ev,
  * dgraph may be NULL for MG_ORDER_REFERENCE and MG_ORDER_GIVEN.           */
 int  mg_plan_order(void* dgraph, const mg_csr_view* q, const mg_opts* opts,
                    uint32_t* order, uint32_t* k);
+/* Orders of nq queries at once (orders[q*MG_MAX_QUERY_VERTICES + i]); with
+ * MG_ORDER_LEARNED one inference launch scores every candidate prefix of the
+ * whole set.  Same plan as nq calls of WOJExecutionPlan::
+ * GenerateWOJExecutionPlan (core/data_structures/woj_exec_plan.cuh:33-50). */
+int  mg_plan_orders(void* dgraph, const mg_csr_view* const* qs, uint32_t nq,
+                    const mg_opts* opts, uint32_t* orders);
 
 /* ---- device graph ------------------------------------------------------- */
 /* Uploads a data graph to `device` and builds the derived indices

@@ -135,6 +135,7 @@ _SIGS = {
     "mg_graph_get_info": (C.c_int, [_VP, C.POINTER(GraphInfo)]),
     "mg_graph_upload_ex": (C.c_int, [_PV, C.c_int, C.POINTER(UploadOpts), _PVP]),
     "mg_selftest_wait_timeout": (C.c_int, [_VP, _PV, C.c_uint32, C.POINTER(C.c_int)]),
+    "mg_plan_orders": (C.c_int, [_VP, C.POINTER(_PV), C.c_uint32, C.POINTER(Opts), P32]),
     "mg_subiso_count": (C.c_int, [_VP, _PV, C.POINTER(Opts), _PU64]),
     "mg_subiso_count_ex": (C.c_int, [_VP, _PV, C.POINTER(Opts), _PU64, C.POINTER(Stats)]),
     "mg_subiso_emit": (C.c_int, [_VP, _PV, C.POINTER(Opts), P32, C.c_uint64, _PU64]),

@@ -27,8 +27,6 @@
 #include <cstring>
 #include <numeric>
 
-#include <cub/cub.cuh>
-
 #include "mg_device.cuh"
 
 namespace mg {
@@ -1482,31 +1480,103 @@ __global__ void k_rows_out(uint32_t* const* cols, const uint32_t* __restrict__ p
   }
 }
 
+// ---- emit: stable LSD radix sort of (key, index) pairs ----------------------
+// One pass sorts by one 8-bit digit of the 32-bit keys:
+//   k_rs_hist    per-tile digit counts, stored digit-major (count[d * nt + t]);
+//   scan         exclusive offsets over that digit-major order (k_scan_*);
+//   k_rs_scatter each tile re-reads its keys in order and writes key and index
+//                to offset[d * nt + t] + (earlier keys of the tile with digit d).
+// Four passes order the keys; rows are sorted column by column from the last
+// one, and stability keeps earlier passes' order among equal keys.
+constexpr int RS_TILE = 2048;        // keys per tile (8 rounds of 256)
+constexpr int RS_BLOCK = 256;
+
+__global__ void __launch_bounds__(RS_BLOCK) k_rs_hist(const uint32_t* __restrict__ keys,
+                                                     uint64_t n, uint32_t shift, uint32_t nt,
+                                                     uint32_t* counts) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const uint64_t base = uint64_t(blockIdx.x) * RS_TILE;
+  for (uint32_t j = threadIdx.x; j < RS_TILE; j += RS_BLOCK) {
+    const uint64_t i = base + j;
+    if (i < n) atomicAdd(&h[(keys[i] >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  counts[uint64_t(threadIdx.x) * nt + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(RS_BLOCK) k_rs_scatter(const uint32_t* __restrict__ keys,
+                                                        const uint32_t* __restrict__ vals,
+                                                        uint64_t n, uint32_t shift, uint32_t nt,
+                                                        const uint64_t* __restrict__ offs,
+                                                        uint32_t* keys_out, uint32_t* vals_out) {
+  __shared__ uint32_t run[256];               // keys of each digit placed so far
+  __shared__ uint32_t wc[RS_BLOCK / 32][256];  // this round: keys of each digit per warp
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  run[threadIdx.x] = 0;
+  for (int w = 0; w < RS_BLOCK / 32; ++w) wc[w][threadIdx.x] = 0;
+  __syncthreads();
+  const uint64_t base = uint64_t(blockIdx.x) * RS_TILE;
+  for (uint32_t r0 = 0; r0 < RS_TILE; r0 += RS_BLOCK) {
+    const uint64_t i = base + r0 + threadIdx.x;
+    const bool valid = i < n;
+    const uint32_t key = valid ? keys[i] : 0u;
+    const uint32_t d = (key >> shift) & 255u;
+    // lanes of this warp holding the same digit, in lane (= input) order
+    const uint32_t peers = __match_any_sync(FULL, valid ? d : 256u + lane);
+    const uint32_t below = __popc(peers & lanemask_lt());
+    if (valid && below == 0) wc[warp][d] = __popc(peers);
+    __syncthreads();
+    if (valid) {
+      uint32_t pos = run[d] + below;
+      for (uint32_t w = 0; w < warp; ++w) pos += wc[w][d];
+      const uint64_t o = offs[uint64_t(d) * nt + blockIdx.x] + pos;
+      keys_out[o] = key;
+      vals_out[o] = vals[i];
+    }
+    __syncthreads();
+    uint32_t add = 0;
+    for (int w = 0; w < RS_BLOCK / 32; ++w) {
+      add += wc[w][threadIdx.x];
+      wc[w][threadIdx.x] = 0;
+    }
+    run[threadIdx.x] += add;
+    __syncthreads();
+  }
+}
+
 static int sort_and_copy(DevGraph* dg, const EmitBuf& eb, uint32_t k, uint64_t n, uint32_t* h_rows,
                          uint64_t n_copy) {
   cudaStream_t st = dg->stream;
   if (n == 0 || n_copy == 0) return MG_OK;
-  uint32_t *perm_a, *perm_b, *keys_a, *keys_b;
+  const uint32_t nt = uint32_t((n + RS_TILE - 1) / RS_TILE);
+  const uint64_t nc = uint64_t(nt) * 256;  // digit-major counts of one pass
+  if (nc >= (1ull << 32)) return set_error(MG_E_LIMIT, "emit sort of %llu rows", (unsigned long long)n);
+  uint32_t *perm_a, *perm_b, *keys_a, *keys_b, *cnt;
+  uint64_t *offs, *bsum;
   MG_CK(cudaMallocAsync((void**)&perm_a, n * 4, st));
   MG_CK(cudaMallocAsync((void**)&perm_b, n * 4, st));
   MG_CK(cudaMallocAsync((void**)&keys_a, n * 4, st));
   MG_CK(cudaMallocAsync((void**)&keys_b, n * 4, st));
+  MG_CK(cudaMallocAsync((void**)&cnt, nc * 4, st));
+  MG_CK(cudaMallocAsync((void**)&offs, (nc + 1) * 8, st));
+  const uint32_t nb = uint32_t((nc + SCAN_TILE - 1) / SCAN_TILE);
+  MG_CK(cudaMallocAsync((void**)&bsum, (uint64_t(nb) + 1) * 8, st));
   k_iota<<<grid_for(n, 256, 4096), 256, 0, st>>>(perm_a, uint32_t(n));
-  int end_bit = 1;
-  while (end_bit < 32 && (uint64_t(dg->info.n) > (1ull << end_bit))) ++end_bit;
-  // Global ids may exceed n when the graph uses non-identity ids.
-  end_bit = 32;
-  size_t tmp_bytes = 0;
-  MG_CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys_a, keys_b, perm_a, perm_b,
-                                        int(n), 0, end_bit, st));
-  void* tmp;
-  MG_CK(cudaMallocAsync(&tmp, std::max<size_t>(16, tmp_bytes), st));
   for (int c = int(k) - 1; c >= 0; --c) {
     k_gather<<<grid_for(n, 256, 4096), 256, 0, st>>>(eb.col[c], perm_a, keys_a, n);
-    MG_CK(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys_a, keys_b, perm_a, perm_b, int(n),
-                                          0, end_bit, st));
-    std::swap(perm_a, perm_b);
+    for (uint32_t shift = 0; shift < 32; shift += 8) {
+      k_rs_hist<<<nt, RS_BLOCK, 0, st>>>(keys_a, n, shift, nt, cnt);
+      k_scan_reduce<<<nb, 256, 0, st>>>(cnt, uint32_t(nc), bsum);
+      k_scan_bsum<<<1, 1024, 0, st>>>(bsum, nb, offs + nc);
+      k_scan_apply<<<nb, 256, 0, st>>>(cnt, uint32_t(nc), bsum, offs);
+      k_rs_scatter<<<nt, RS_BLOCK, 0, st>>>(keys_a, perm_a, n, shift, nt, offs, keys_b, perm_b);
+      std::swap(keys_a, keys_b);
+      std::swap(perm_a, perm_b);
+    }
   }
+  MG_CK(cudaGetLastError());
   uint32_t** d_cols;
   MG_CK(cudaMallocAsync((void**)&d_cols, sizeof(uint32_t*) * MAXK, st));
   MG_CK(cudaMemcpyAsync(d_cols, eb.col, sizeof(uint32_t*) * MAXK, cudaMemcpyHostToDevice, st));
@@ -1515,13 +1585,9 @@ static int sort_and_copy(DevGraph* dg, const EmitBuf& eb, uint32_t k, uint64_t n
   k_rows_out<<<grid_for(n_copy * k, 256, 4096), 256, 0, st>>>(d_cols, perm_a, k, d_rows, n_copy);
   MG_CK(cudaMemcpyAsync(h_rows, d_rows, n_copy * k * 4, cudaMemcpyDeviceToHost, st));
   MG_CK(cudaStreamSynchronize(st));
-  cudaFreeAsync(perm_a, st);
-  cudaFreeAsync(perm_b, st);
-  cudaFreeAsync(keys_a, st);
-  cudaFreeAsync(keys_b, st);
-  cudaFreeAsync(tmp, st);
-  cudaFreeAsync(d_cols, st);
-  cudaFreeAsync(d_rows, st);
+  for (void* p : {(void*)perm_a, (void*)perm_b, (void*)keys_a, (void*)keys_b, (void*)cnt,
+                  (void*)offs, (void*)bsum, (void*)d_cols, (void*)d_rows})
+    cudaFreeAsync(p, st);
   MG_CK(cudaStreamSynchronize(st));
   return MG_OK;
 }
@@ -2128,6 +2194,39 @@ int mg_subiso_batch_count_orders(void* dgraph, const mg_csr_view* const* qs, uin
   if (!qs || !counts || nq == 0) return mg::set_error(MG_E_ARG, "null argument or empty batch");
   try {
     return mg::subiso_batch(dg, qs, nq, opts, counts, st, orders, level_rows);
+  } catch (const std::bad_alloc&) {
+    return mg::set_error(MG_E_OOM, "host allocation failed");
+  }
+}
+
+int mg_plan_orders(void* dgraph, const mg_csr_view* const* qs, uint32_t nq, const mg_opts* opts,
+                   uint32_t* orders) {
+  MG_ENTRY(dgraph);
+  if (!qs || !orders || nq == 0) return mg::set_error(MG_E_ARG, "null argument or empty batch");
+  try {
+    const mg_opts o = mg::resolve_opts(opts);
+    std::vector<mg::QueryGraph> Q(nq);
+    for (uint32_t i = 0; i < nq; ++i) {
+      int rc = mg::normalise_query(qs[i], &Q[i]);
+      if (rc) return mg::set_error(rc, "query %u: %s", i, mg::last_error_cstr());
+    }
+    std::memset(orders, 0, uint64_t(nq) * MG_MAX_QUERY_VERTICES * 4);
+    if (o.order == MG_ORDER_LEARNED && o.model) {
+      int rc = mg::ensure_full_stats(dg);
+      if (rc) return rc;
+      std::vector<const mg::QueryGraph*> qp(nq);
+      for (uint32_t i = 0; i < nq; ++i) qp[i] = &Q[i];
+      std::vector<std::array<uint32_t, MG_MAX_QUERY_VERTICES>> ord;
+      if ((rc = mg::order_learned_batch(o.model, qp, dg->stats, ord))) return rc;
+      for (uint32_t i = 0; i < nq; ++i)
+        std::memcpy(orders + uint64_t(i) * MG_MAX_QUERY_VERTICES, ord[i].data(), Q[i].k * 4);
+      return MG_OK;
+    }
+    for (uint32_t i = 0; i < nq; ++i) {
+      int rc = mg::choose_order(dg, Q[i], o, orders + uint64_t(i) * MG_MAX_QUERY_VERTICES);
+      if (rc) return rc;
+    }
+    return MG_OK;
   } catch (const std::bad_alloc&) {
     return mg::set_error(MG_E_OOM, "host allocation failed");
   }

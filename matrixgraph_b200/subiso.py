@@ -154,6 +154,15 @@ class DeviceGraph:
     def plan_order(self, q: CSRGraph, order="reference", **kw) -> list[int]:
         return plan_order(q, order=order, graph=self, **kw)
 
+    def plan_orders(self, qs: Sequence[CSRGraph], order="reference", **kw) -> list[list[int]]:
+        """Orders of many queries in one call (one inference launch when learned)."""
+        o, keep = make_opts(order=order, **kw)
+        nq = len(qs)
+        arr = (C.POINTER(L.CsrView) * nq)(*[C.pointer(q.view) for q in qs])
+        out = np.zeros((nq, L.MG_MAX_QUERY_VERTICES), dtype=np.uint32)
+        L.check(L.lib.mg_plan_orders(self.handle, arr, nq, C.byref(o), out.ctypes.data_as(L.P32)))
+        return [out[i, :q.n].tolist() for i, q in enumerate(qs)]
+
     def free(self) -> None:
         if self.handle:
             L.lib.mg_graph_free(self.handle)

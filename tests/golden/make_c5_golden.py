@@ -6,11 +6,15 @@ generator by tests/test_oracle_generators.py).  bench.py counts the same
 samples on the GPU and requires equal counts (and equal sorted rows, through
 their SHA-256, where the sample has at most 20,000 matches).
 
-Each sample is the low-degree end of the query's level-0 bucket, [nb - r, nb),
-with r the largest power of two (up to 2^16) whose oracle count stays at or
-below 10^6 and finishes within 10 s; each attempt runs in a forked child that
-is killed at 30 s (a vertex near a hub can take the oracle minutes).  Needs
-about 40 GB of host memory; a few minutes on 8 cores.
+Each sample is first the low-degree end of the query's level-0 bucket,
+[nb - r, nb), with r the largest power of two (up to 2^16) whose oracle count
+stays at or below 10^6 and finishes within 10 s.  When that sample has no
+match, systematic samples over the bucket past its first 1% (positions
+nb/100, nb/100 + s, ... for s = nb/8, nb/16, ... down to nb/4096) are tried
+and the first with a match under the same limits is kept.  Each attempt runs
+in a forked child that is killed at 30 s (a vertex near a hub can take the
+oracle minutes).  Needs about 40 GB of host memory; several minutes on 8
+cores.
 
     python tests/golden/make_c5_golden.py [n_queries]
 """
@@ -95,12 +99,27 @@ def main():
             if dt > 10:
                 break
             r *= 2
+        if best is None or best["count"] == 0:
+            j = 3
+            while nb >> j >= 1 and j <= 12:
+                b, st = nb // 100, max(1, nb >> j)
+                t1 = time.perf_counter()
+                res = timed(lambda: O.count(og, oq, order=order, threads=threads,
+                                            root_range=(b, nb), root_step=st), 30)
+                dt = time.perf_counter() - t1
+                if res is None or res["count"] > 10 ** 6:
+                    break
+                if res["count"] > 0:
+                    best = {"begin": b, "end": nb, "step": st, "count": res["count"],
+                            "level_rows": res["level_rows"], "oracle_seconds": dt}
+                    break
+                j += 1
         rec = {"q": q, "k": k, "edges": edges, "labels": labels, "order": order, "bucket": nb}
         if best is not None:
             rec.update(best)
             if best["count"] <= 20000:
                 rows = O.emit(og, oq, order=order, cap=best["count"],
-                              root_range=(best["begin"], best["end"]))
+                              root_range=(best["begin"], best["end"]), root_step=best["step"])
                 rec["rows_sha256"] = hashlib.sha256(
                     np.ascontiguousarray(rows, dtype="<u4").tobytes()).hexdigest()
         out["queries"].append(rec)

@@ -436,3 +436,35 @@ def test_bounded_device_wait_times_out_and_context_stays_usable(c1):
         assert status.value == L.MG_E_TIMEOUT, limit
     qs = [mg.query_random(g, 3 + i % 4, 0.3, seed=7000 + i) for i in range(16)]
     assert dg.batch_count(qs).tolist() == [dg.count(x) for x in qs]
+
+
+def test_emit_sort_with_large_global_ids():
+    """Emitted rows are sorted by the library's own radix sort over the
+    global ids; ids above 2^24 exercise every digit pass, and the rows equal
+    the oracle's sorted rows."""
+    rng = np.random.default_rng(31)
+    n = 1500
+    edges, labels = random_graph(rng, n, 0.02, 2)
+    g = graph(n, edges, labels)
+    gid = (300_000_000 - 7 * np.arange(n)).astype(np.uint32)
+    ge = g.array("globalid")
+    oe = g.array("out_edges")
+    ie = g.array("in_edges")
+    same = oe.ctypes.data == ie.ctypes.data
+    oe[:] = gid[oe]
+    if not same:
+        ie[:] = gid[ie]
+    ge[:] = gid
+    g.view.max_vid = int(gid.max())
+    g.view.min_vid = int(gid.min())
+    g.view.edges_globalid_by_localid = None
+    g.view.localid_by_globalid = None
+    dg = mg.DeviceGraph(g)
+    try:
+        for qe, ql in (([(0, 1), (1, 2), (2, 0)], [0, 1, 0]), ([(0, 1), (1, 2)], [1, 0, 1])):
+            q = mg.CSRGraph.query(3, qe, ql)
+            rows = dg.emit(q)
+            assert len(rows) > 1000
+            assert np.array_equal(rows, oracle_rows(g, q))
+    finally:
+        dg.free()
