@@ -420,10 +420,24 @@ static int upload(const mg_csr_view* v, int device, const mg_upload_opts& uo, De
   dg->info.n = n;
   dg->info.device = device;
 
-  // Label compaction (host): distinct raw labels, ascending.
-  std::vector<uint32_t> vals(v->labels, v->labels + n);
-  std::sort(vals.begin(), vals.end());
-  vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
+  // Label compaction (host): distinct raw labels, ascending.  Small label
+  // values (the usual case) are collected with a presence table in one pass;
+  // other values by sorting a copy.
+  std::vector<uint32_t> vals;
+  {
+    uint32_t lmax = 0;
+    for (uint32_t i = 0; i < n; ++i) lmax = std::max(lmax, v->labels[i]);
+    if (lmax < (1u << 22)) {
+      std::vector<uint8_t> seen(uint64_t(lmax) + 1, 0);
+      for (uint32_t i = 0; i < n; ++i) seen[v->labels[i]] = 1;
+      for (uint32_t x = 0; x <= lmax; ++x)
+        if (seen[x]) vals.push_back(x);
+    } else {
+      vals.assign(v->labels, v->labels + n);
+      std::sort(vals.begin(), vals.end());
+      vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
+    }
+  }
   if (vals.size() > MG_MAX_LABELS)
     return set_error(MG_E_LIMIT, "%zu distinct labels; at most %d supported", vals.size(),
                      MG_MAX_LABELS);
@@ -438,9 +452,18 @@ static int upload(const mg_csr_view* v, int device, const mg_upload_opts& uo, De
   dg->stats.label_values = vals;
   std::vector<uint32_t> lab(n);
   std::vector<uint64_t> cnt(L, 0);
-  for (uint32_t i = 0; i < n; ++i) {
-    lab[i] = uint32_t(std::lower_bound(vals.begin(), vals.end(), v->labels[i]) - vals.begin());
-    cnt[lab[i]]++;
+  if (vals.back() < (1u << 22)) {
+    std::vector<uint32_t> to_compact(uint64_t(vals.back()) + 1, 0);
+    for (uint32_t c = 0; c < L; ++c) to_compact[vals[c]] = c;
+    for (uint32_t i = 0; i < n; ++i) {
+      lab[i] = to_compact[v->labels[i]];
+      cnt[lab[i]]++;
+    }
+  } else {
+    for (uint32_t i = 0; i < n; ++i) {
+      lab[i] = uint32_t(std::lower_bound(vals.begin(), vals.end(), v->labels[i]) - vals.begin());
+      cnt[lab[i]]++;
+    }
   }
   dg->stats.label_count = cnt;
   dg->h_bucket_off.assign(L + 1, 0);
