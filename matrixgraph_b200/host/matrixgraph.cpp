@@ -2,6 +2,7 @@
 
 #include <chrono>
 #include <fstream>
+#include <sstream>
 #include <iostream>
 
 namespace matrixgraph {
@@ -86,13 +87,39 @@ void SubIso::Write() const {
 
 BatchSubIso::BatchSubIso(const std::vector<std::string>& pattern_paths,
                          const std::string& data_graph_path, const std::string& output_path,
-                         int order, const std::string& model_path, int device)
+                         int order, const std::string& model_path, int device,
+                         const std::string& tune_path)
     : pattern_paths_(pattern_paths),
       data_graph_path_(data_graph_path),
       output_path_(output_path),
       model_path_(model_path),
+      tune_path_(tune_path),
       order_(order),
       device_(device) {}
+
+namespace {
+struct TuneRow {
+  uint32_t k_lo, k_hi, lanes, probe_min, grab;
+};
+
+// Rows of an autotuner table whose signature is this graph's.
+std::vector<TuneRow> ReadTuneTable(const std::string& path, const mg_graph_info& gi) {
+  std::ifstream f(path);
+  if (!f) throw Error(MG_E_IO, "cannot read the tune table " + path);
+  const std::string sig = "n" + std::to_string(gi.n) + ".m" + std::to_string(gi.m_out) + ".L" +
+                          std::to_string(gi.n_labels) + ".d" + std::to_string(gi.max_degree);
+  std::vector<TuneRow> rows;
+  for (std::string line; std::getline(f, line);) {
+    if (line.empty() || line[0] == '#') continue;
+    std::istringstream in(line);
+    std::string s;
+    TuneRow r{};
+    if ((in >> s >> r.k_lo >> r.k_hi >> r.lanes >> r.probe_min >> r.grab) && s == sig)
+      rows.push_back(r);
+  }
+  return rows;
+}
+}  // namespace
 
 BatchSubIso::~BatchSubIso() {
   for (void* o : p_owner_)
@@ -121,10 +148,48 @@ void BatchSubIso::Run() {
     for (auto& v : p_) qs.push_back(&v);
     counts_.assign(qs.size(), 0);
     mg_stats st;
-    rc = mg_subiso_batch_count_ex(dg, qs.data(), uint32_t(qs.size()), &o, counts_.data(), &st);
-    if (rc == MG_OK)
-      std::cout << "[BatchSubIso] " << qs.size() << " patterns, device " << st.device_ms
-                << " ms, " << st.launches << " launches" << std::endl;
+    std::vector<TuneRow> tune;
+    if (!tune_path_.empty()) {
+      mg_graph_info gi;
+      Check(mg_graph_get_info(dg, &gi));
+      tune = ReadTuneTable(tune_path_, gi);
+    }
+    if (tune.empty()) {
+      rc = mg_subiso_batch_count_ex(dg, qs.data(), uint32_t(qs.size()), &o, counts_.data(),
+                                    &st);
+      if (rc == MG_OK)
+        std::cout << "[BatchSubIso] " << qs.size() << " patterns, device " << st.device_ms
+                  << " ms, " << st.launches << " launches" << std::endl;
+    } else {
+      // one batched call per tuned size bucket, then the leftover sizes
+      std::vector<char> done(qs.size(), 0);
+      for (size_t b = 0; b <= tune.size() && rc == MG_OK; ++b) {
+        std::vector<const mg_csr_view*> part;
+        std::vector<size_t> idx;
+        for (size_t i = 0; i < qs.size(); ++i) {
+          const uint32_t k = qs[i]->n;
+          const bool in = b < tune.size() ? (k >= tune[b].k_lo && k <= tune[b].k_hi) : !done[i];
+          if (in && !done[i]) {
+            part.push_back(qs[i]);
+            idx.push_back(i);
+            done[i] = 1;
+          }
+        }
+        if (part.empty()) continue;
+        mg_opts ob = o;
+        if (b < tune.size()) {
+          ob.lanes = tune[b].lanes;
+          ob.probe_min = tune[b].probe_min;
+          ob.grab = tune[b].grab;
+        }
+        std::vector<uint64_t> c(part.size(), 0);
+        rc = mg_subiso_batch_count(dg, part.data(), uint32_t(part.size()), &ob, c.data());
+        for (size_t j = 0; j < idx.size() && rc == MG_OK; ++j) counts_[idx[j]] = c[j];
+      }
+      if (rc == MG_OK)
+        std::cout << "[BatchSubIso] " << qs.size() << " patterns, tuned by " << tune_path_
+                  << std::endl;
+    }
   }
   const std::string msg = rc == MG_OK ? "" : mg_last_error();
   if (dg) mg_graph_free(dg);

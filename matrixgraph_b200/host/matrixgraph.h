@@ -71,9 +71,13 @@ class SubIso {
 // launch).  No counterpart in the reference, whose CLI takes one pattern.
 class BatchSubIso {
  public:
+  // tune_path: an autotuner table (matrixgraph_b200/autotune.py): rows
+  // "signature k_lo k_hi lanes probe_min grab seconds"; the rows of this
+  // graph's signature set the launch options of each query-size bucket.
   BatchSubIso(const std::vector<std::string>& pattern_paths, const std::string& data_graph_path,
               const std::string& output_path, int order = MG_ORDER_REFERENCE,
-              const std::string& model_path = "", int device = 0);
+              const std::string& model_path = "", int device = 0,
+              const std::string& tune_path = "");
   ~BatchSubIso();
   void Run();
 
@@ -81,7 +85,7 @@ class BatchSubIso {
 
  private:
   std::vector<std::string> pattern_paths_;
-  std::string data_graph_path_, output_path_, model_path_;
+  std::string data_graph_path_, output_path_, model_path_, tune_path_;
   int order_, device_;
   std::vector<mg_csr_view> p_;
   std::vector<void*> p_owner_;

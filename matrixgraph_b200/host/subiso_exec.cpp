@@ -3,8 +3,9 @@
 // [-o <output>] [-scheduler CHBL|EvenSplit|RoundRobin] plus
 // [-mode count|emit] [-order reference|heuristic|strong|learned]
 // [-model <order model dir/>] [-batch <file of pattern dirs, one per line>]
-// [-device N].  With -batch, -p is not needed and every pattern is counted
-// in one batched call; -o receives "pattern count" lines.
+// [-device N] [-tune <autotuner table>].  With -batch, -p is not needed and
+// every pattern is counted in batched calls (one per tuned query-size bucket
+// with -tune); -o receives "pattern count" lines.
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
@@ -29,7 +30,7 @@ int main(int argc, char** argv) {
   std::map<std::string, std::string> flags = {
       {"p", ""}, {"g", ""}, {"e", ""}, {"o", ""}, {"scheduler", "CHBL"},
       {"mode", "count"}, {"order", "reference"}, {"device", "0"}, {"batch", ""},
-      {"model", ""}};
+      {"model", ""}, {"tune", ""}};
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i];
     while (!a.empty() && a[0] == '-') a = a.substr(1);
@@ -88,7 +89,7 @@ int main(int argc, char** argv) {
     std::cerr << "Usage: " << argv[0] << " -p <pattern_path/> -g <graph_path/> [-e <edge_list>]"
               << " [-o <output_path>] [-scheduler CHBL] [-mode count|emit]"
               << " [-order reference|strong|learned] [-model <dir/>] [-batch <list>]"
-              << " [-device N]" << std::endl;
+              << " [-device N] [-tune <table>]" << std::endl;
     return EXIT_FAILURE;
   }
   std::cout << "\n=== SubIso Configuration ===\nPattern Graph: " << flags["p"]
@@ -101,7 +102,7 @@ int main(int argc, char** argv) {
     const int device = std::atoi(flags["device"].c_str());
     if (!batch.empty()) {
       matrixgraph::BatchSubIso task(batch, flags["g"], flags["o"], order, flags["model"],
-                                    device);
+                                    device, flags["tune"]);
       system.Run(matrixgraph::kSubIso, &task);
     } else {
       SubIso task(flags["p"], flags["g"], flags["e"], flags["o"], flags["mode"], order, device,

@@ -468,3 +468,40 @@ def test_emit_sort_with_large_global_ids():
             assert np.array_equal(rows, oracle_rows(g, q))
     finally:
         dg.free()
+
+
+def test_subiso_exec_batch_tuned(tmp_path):
+    """subiso_exec -batch, untuned and with an autotuner table (one batched
+    call per tuned size bucket), prints the counts of the Python batch call;
+    the autotuner's trials agree on every count."""
+    import subprocess
+    from matrixgraph_b200 import autotune
+    g = mg.rmat(12, n_labels=4)
+    dg = mg.DeviceGraph(g)
+    qs = [mg.query_random(g, 3 + i % 5, 0.3, seed=4100 + i) for i in range(10)]
+    want = dg.batch_count(qs).tolist()
+    best = autotune.tune(dg, qs, sample=4,
+                         candidates={"lanes": (2, 8), "probe_min": (1, 64), "grab": (0, 4)})
+    assert set(best) == {autotune.bucket_of(q.n) for q in qs}
+    table = str(tmp_path / "tune.txt")
+    autotune.save_table(table, dg, best)
+    loaded = autotune.load_table(table, dg)
+    assert autotune.tuned_batch_count(dg, qs, loaded).tolist() == want
+    g.Write(str(tmp_path / "g") + "/")
+    names = []
+    for i, q in enumerate(qs):
+        q.Write(str(tmp_path / f"p{i}") + "/")
+        names.append(str(tmp_path / f"p{i}") + "/")
+    (tmp_path / "list.txt").write_text("\n".join(names) + "\n")
+    exe = os.path.join(os.path.dirname(mg.__file__), "subiso_exec")
+    for extra in ([], ["-tune", table]):
+        out = tmp_path / "counts.txt"
+        r = subprocess.run([exe, "-g", str(tmp_path / "g") + "/", "-batch",
+                            str(tmp_path / "list.txt"), "-o", str(out), *extra],
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        got = [int(ln.split()[-1]) for ln in out.read_text().splitlines() if ln.strip()]
+        assert got == want, extra
+        if extra:
+            assert "tuned by" in r.stdout
+    dg.free()
