@@ -102,3 +102,67 @@ def test_committed_model_loads_and_keeps_counts_exact(setup):
     for q in qs:
         assert dg.count(q, order="learned", model=model) == dg.count(q)
     model.free()
+
+
+def _numpy_features(g, q):
+    """The order model's per-vertex and per-edge features restated from the
+    CSR arrays (symmetric graph): per compact label the vertex count, mean /
+    maximum / 99th-percentile-bin degree, the number of neighbour labels, and
+    the label-pair edge counts."""
+    lab_raw = g.array("labels").astype(np.int64)
+    values = np.unique(lab_raw)
+    comp = np.searchsorted(values, lab_raw)
+    L = len(values)
+    off = g.array("out_off").astype(np.int64)
+    deg = np.diff(off)
+    nbr_lab = comp[g.array("out_edges").astype(np.int64)]
+    src_lab = np.repeat(comp, deg)
+    pair = np.zeros((L, L), dtype=np.int64)
+    np.add.at(pair, (src_lab, nbr_lab), 1)
+    count = np.bincount(comp, minlength=L)
+    dsum = np.bincount(comp, weights=deg, minlength=L)
+    dmax = np.zeros(L, dtype=np.int64)
+    np.maximum.at(dmax, comp, deg)
+    bins = np.where(deg == 0, 0, np.floor(np.log2(np.maximum(deg, 1))).astype(np.int64) + 1)
+    p99 = np.zeros(L)
+    for l in range(L):
+        h = np.bincount(bins[comp == l], minlength=33)
+        target = count[l] - count[l] // 100
+        b = int(np.argmax(np.cumsum(h) >= target))
+        p99[l] = 0.0 if b == 0 else float((1 << b) - 1)
+    k = q.n
+    qlab = np.searchsorted(values, q.array("labels").astype(np.int64))
+    qoff, qadj = q.array("out_off"), q.array("out_edges")
+    nb = [0] * k
+    for u in range(k):
+        for w in qadj[qoff[u]:qoff[u + 1]]:
+            if w != u:
+                nb[u] |= 1 << int(w)
+                nb[int(w)] |= 1 << u
+    x = np.zeros((16, 8), dtype=np.float32)
+    e = np.zeros((16, 16), dtype=np.float32)
+    for u in range(k):
+        l = qlab[u]
+        x[u] = [np.log1p(count[l]) / 16.0, np.log1p(dsum[l] / count[l]) / 8.0,
+                np.log1p(dmax[l]) / 16.0, np.log1p(p99[l]) / 12.0,
+                np.count_nonzero(pair[l]) / L, 0.0, bin(nb[u]).count("1") * 0.125,
+                np.log1p(g.n) / 20.0]
+        for w in range(k):
+            if (nb[u] >> w) & 1:
+                e[u, w] = np.log1p(pair[l, qlab[w]]) / 24.0
+    return x, e, np.array(nb + [0] * (16 - k), dtype=np.uint32)
+
+
+def test_features_match_a_numpy_restatement():
+    """The label statistics the GPU computes (k_label_stats) and the features
+    built from them equal a numpy computation from the CSR arrays."""
+    g = mg.rmat(12, n_labels=7)
+    dg = mg.DeviceGraph(g)
+    for i in range(8):
+        q = mg.query_random(g, 3 + i % 6, 0.4, seed=500 + i)
+        x, e, adj = OM.features(dg, q)
+        wx, we, wadj = _numpy_features(g, q)
+        assert np.array_equal(adj, wadj), i
+        assert np.allclose(x, wx, rtol=1e-6, atol=1e-7), (i, x[:q.n], wx[:q.n])
+        assert np.allclose(e, we, rtol=1e-6, atol=1e-7), i
+    dg.free()
