@@ -22,12 +22,13 @@
     python -m matrixgraph_b200.workloads eval-batch MODEL_DIR/ OUT.json
 
 Learned order: training queries are random connected queries with k uniform
-in 6..10 (seeds from 100000) on the scale-20 graph, kept when the reference
-order needs at most TRAIN_BUDGET elements; the enumerator records P_i for the
-reference order and 8 random connected orders of each (per-query budget).
-Held-out queries use seeds from 200000 on the scale-22 graph.  Both
-selections stop after a fixed time; the kept seeds are committed with the
-model (data/order_train_record.json, data/order_eval.json).
+in 6..10 (seeds from 100000, taken in order) on the scale-20 graph; the
+enumerator records P_i for the reference order and 8 random connected orders
+of each under a per-run budget of TRAIN_BUDGET elements, and every run that
+finishes gives one sample per prefix (a heavy query enters through the
+orders that finish, whatever its reference order costs).  The seeds and run
+totals are committed with the model (data/order_train_record.json).
+Held-out queries use seeds from 200000 on the scale-22 graph.
 """
 from __future__ import annotations
 
@@ -184,16 +185,16 @@ def select_queries(dg, g, make, first_seed, n, budget, max_candidates, log=None,
     return kept, dropped
 
 
-def train_order(outdir: str, n_train: int = 4000, n_random: int = 8, epochs: int = 60,
-                log=print, select_seconds: float = 200.0):
+def train_order(outdir: str, n_train: int = 8000, n_random: int = 8, epochs: int = 30,
+                log=print):
     import time
     from .order_model import OrderModel, record_prefix_counts
     t0 = time.time()
     g = rmat_graph(TRAIN_SCALE)
     dg = DeviceGraph(g)
-    kept, dropped = select_queries(dg, g, learned_query, TRAIN_FIRST_SEED, n_train, TRAIN_BUDGET,
-                                   40 * n_train, log, max_seconds=select_seconds)
-    log(f"train queries: kept {len(kept)} dropped {dropped} ({time.time() - t0:.1f}s)")
+    kept = [{"seed": s, "k": learned_k(s)} for s in range(TRAIN_FIRST_SEED,
+                                                            TRAIN_FIRST_SEED + n_train)]
+    dropped = 0
     qs = [learned_query(g, r["seed"]) for r in kept]
     (sq, sm, st), records = record_prefix_counts(dg, qs, n_random, TRAIN_BUDGET, seed=7)
     censored = sum(1 for r in records if r[2] == 2 ** 64 - 1)
@@ -208,9 +209,11 @@ def train_order(outdir: str, n_train: int = 4000, n_random: int = 8, epochs: int
     log(f"loss: init {l0:.3f} train {ltr:.3f} validation {lval:.3f} ({time.time() - t0:.1f}s)")
     os.makedirs(os.path.join(outdir, "order_model"), exist_ok=True)
     model.save(os.path.join(outdir, "order_model") + "/")
+    finished = sorted({r[0] for r in records if r[2] != 2 ** 64 - 1})
     rec = {"graph": f"rmat scale {TRAIN_SCALE} (workloads.rmat_graph)", "budget": TRAIN_BUDGET,
-           "first_seed": TRAIN_FIRST_SEED, "seeds": [r["seed"] for r in kept],
-           "k": [r["k"] for r in kept], "dropped": dropped, "runs": len(records),
+           "first_seed": TRAIN_FIRST_SEED, "n_queries": len(kept),
+           "queries_with_a_finished_run": len(finished), "dropped": dropped,
+           "runs": len(records),
            "censored_runs": censored, "samples": int(len(sq)), "epochs": epochs,
            "loss_init": l0, "loss_train": ltr, "loss_validation": lval,
            "seconds": time.time() - t0}
@@ -326,7 +329,7 @@ def eval_batch(model_dir: str, out_path: str, log=print):
 
 def main(argv):
     if len(argv) >= 2 and argv[0] == "train-order":
-        train_order(argv[1], n_train=int(argv[2]) if len(argv) > 2 else 4000)
+        train_order(argv[1], n_train=int(argv[2]) if len(argv) > 2 else 8000)
         return 0
     if len(argv) >= 3 and argv[0] == "eval-order":
         eval_order(argv[1], argv[2], n_eval=int(argv[3]) if len(argv) > 3 else 2000)

@@ -104,6 +104,39 @@ def test_committed_model_loads_and_keeps_counts_exact(setup):
     model.free()
 
 
+def test_committed_model_cuts_work_on_held_out_queries():
+    """The committed network's orders expand fewer candidate elements in total
+    than the reference order on held-out queries (seeds from 200000, k 6-10)
+    of the scale-20 graph; element counts are exact, so the check is
+    deterministic.  Queries past the budget under either order are skipped."""
+    from matrixgraph_b200 import _lib as L
+    from matrixgraph_b200 import workloads as W
+    if not os.path.exists(MODEL_DIR + "embedding.bin"):
+        pytest.skip("no trained model committed")
+    g = W.rmat_graph(20)
+    dg = mg.DeviceGraph(g)
+    model = OM.OrderModel.load(MODEL_DIR)
+    qs = [W.learned_query(g, W.EVAL_FIRST_SEED + i) for i in range(96)]
+    ref = dg.plan_orders(qs, order="reference")
+    lrn = dg.plan_orders(qs, order="learned", model=model)
+    el_ref = el_lrn = both = 0
+    for q, ro, lo in zip(qs, ref, lrn):
+        try:
+            c1, s1 = dg.count(q, stats=True, given_order=ro, max_elements=1 << 27)
+            c2, s2 = dg.count(q, stats=True, given_order=lo, max_elements=1 << 27)
+        except L.MGError as e:
+            assert e.code == L.MG_E_LIMIT
+            continue
+        assert c1 == c2
+        el_ref += s1["elements"]
+        el_lrn += s2["elements"]
+        both += 1
+    model.free()
+    dg.free()
+    assert both >= 48, both
+    assert el_lrn < el_ref, (el_lrn, el_ref)
+
+
 def _numpy_features(g, q):
     """The order model's per-vertex and per-edge features restated from the
     CSR arrays (symmetric graph): per compact label the vertex count, mean /
