@@ -124,6 +124,9 @@ typedef struct mg_opts {
                                 a single-query call above it returns
                                 MG_E_LIMIT; in a batch it applies per query
                                 and a query above it reports UINT64_MAX      */
+  void*    matrix_filter;    /* lossy learned candidate filter
+                                (mg_matrix_filter_load), single-query count
+                                and emit only; NULL = off (exact)            */
 } mg_opts;
 
 #define MG_LANES_SHARED 0xFFFFFFFFu
@@ -368,6 +371,28 @@ int  mg_selftest_wait_timeout(void* dgraph, const mg_csr_view* q, uint32_t spin_
  * cleared at the start of each call); calls are serialised by a process-wide
  * lock, since calls that overlapped on the GPU would race on the array.    */
 #define MG_NOALLOC_SCRATCH_BYTES (16u << 20)
+/* ---- lossy learned candidate filter (MatrixFilter) ---------------------
+ * Replaces the reference's MatrixFilter (core/task/cpu_task/cpu_subiso.cu:
+ * 237-277) with its CPU MLP helpers (core/task/gpu_task/kernel/
+ * kernel_matrix_ops.cu:431-509).  dirs[0..5] are six matrices in the
+ * reference's container (<dir>meta.yaml with x and y, <dir>embedding.bin
+ * float32 row-major; core/data_structures/matrix.cu:12-35), in the order of
+ * the reference's -m1..-m6: query-vertex embeddings (k rows x dim),
+ * data-vertex embeddings (n rows x dim, row = local vertex id), W1 (hidden
+ * rows x dim), b1 (hidden values), W2 (hidden x 1), b2 (1 value); hidden is
+ * at most 64 and dim at most 1024.  A candidate v of query vertex u is
+ * rejected when sigmoid(W2 . relu(W1 . (e_u - e_v)^2 + b1) + b2) < 0.1, with
+ * every product and sum rounded to float32 in the reference's order.  With
+ * mg_opts.matrix_filter set, the level-0 candidates (the first vertex of the
+ * matching order) are filtered; counts then lose the matches of rejected
+ * roots.  Off by default, as in the reference's CLI. */
+int  mg_matrix_filter_load(const char* const dirs[6], int device, void** filter);
+void mg_matrix_filter_free(void* filter);
+/* keep[i] = 1 when the filter keeps (u, v[i]); host arrays; u < k rows of
+ * dirs[0], every v[i] < n rows of dirs[1]. */
+int  mg_matrix_filter_keep(void* filter, uint32_t u, const uint32_t* v, uint64_t nv,
+                           uint8_t* keep);
+
 int  mg_subiso_count_noalloc(void* dgraph, const mg_csr_view* q, const mg_opts* opts,
                              uint64_t* count);
 

@@ -10,7 +10,9 @@ from .graph import (SHAPES, CSRGraph, chung_lu, gen_labels, query_edges,  # noqa
 from .subiso import (DeviceGraph, MatrixGraph, SchedulerType, SubIso, TaskType,  # noqa: F401
                      level0_sizes, make_opts, plan_order, shard_roots,
                      shard_strided)
+from .matrix_filter import MatrixFilter  # noqa: F401
 
 __all__ = ["MGError", "CSRGraph", "DeviceGraph", "SubIso", "MatrixGraph", "TaskType",
            "SchedulerType", "chung_lu", "rmat", "query_walk", "query_random", "gen_labels",
-           "plan_order", "shard_roots", "shard_strided", "level0_sizes", "SHAPES", "query_edges", "make_opts"]
+           "plan_order", "shard_roots", "shard_strided", "level0_sizes", "SHAPES", "query_edges", "make_opts",
+           "MatrixFilter"]

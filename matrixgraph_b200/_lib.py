@@ -64,7 +64,7 @@ class Opts(C.Structure):
                 ("kernel_events", C.c_uint32), ("mem_budget_bytes", C.c_uint64),
                 ("root_begin", C.c_uint64), ("root_end", C.c_uint64),
                 ("no_tail", C.c_uint32), ("lanes", C.c_uint32),
-                ("max_elements", C.c_uint64)]
+                ("max_elements", C.c_uint64), ("matrix_filter", C.c_void_p)]
 
 
 class Stats(C.Structure):
@@ -136,6 +136,10 @@ _SIGS = {
     "mg_graph_upload_ex": (C.c_int, [_PV, C.c_int, C.POINTER(UploadOpts), _PVP]),
     "mg_selftest_wait_timeout": (C.c_int, [_VP, _PV, C.c_uint32, C.POINTER(C.c_int)]),
     "mg_plan_orders": (C.c_int, [_VP, C.POINTER(_PV), C.c_uint32, C.POINTER(Opts), P32]),
+    "mg_matrix_filter_load": (C.c_int, [C.POINTER(C.c_char_p), C.c_int, C.POINTER(C.c_void_p)]),
+    "mg_matrix_filter_free": (None, [_VP]),
+    "mg_matrix_filter_keep": (C.c_int, [_VP, C.c_uint32, P32, C.c_uint64,
+                                        C.POINTER(C.c_uint8)]),
     "mg_subiso_count": (C.c_int, [_VP, _PV, C.POINTER(Opts), _PU64]),
     "mg_subiso_count_ex": (C.c_int, [_VP, _PV, C.POINTER(Opts), _PU64, C.POINTER(Stats)]),
     "mg_subiso_emit": (C.c_int, [_VP, _PV, C.POINTER(Opts), P32, C.c_uint64, _PU64]),

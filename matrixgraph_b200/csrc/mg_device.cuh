@@ -115,6 +115,21 @@ struct DevGraph {
 
 int ensure_full_stats(DevGraph* dg);
 
+// Makes device d current for a scope and restores the caller's device.
+struct DeviceGuard {
+  int prev = 0;
+  explicit DeviceGuard(int d) {
+    cudaGetDevice(&prev);
+    cudaSetDevice(d);
+  }
+  ~DeviceGuard() { cudaSetDevice(prev); }
+};
+
+// Keep bits (ceil(n/32) words) of the vertices of label bucket `lab` for query
+// vertex u under a matrix filter (mg_matrix_filter.cu); synchronises st.
+int matrix_filter_roots(void* filter, const DevGraph* dg, uint32_t u, uint32_t lab,
+                        uint32_t* bits, cudaStream_t st);
+
 #define MG_CK(call)                                                          \
   do {                                                                       \
     cudaError_t _e = (call);                                                 \

@@ -14,7 +14,8 @@
 //     the driving lengths into an element index space;
 //   * the expand kernel assigns one element (row, driving entry) per thread,
 //     so hub rows spread over many warps; the other backward slices are
-//     probed by binary search, injectivity is checked against the row, the
+//     probed in the hub bitmap when their vertex is a hub, else by binary
+//     search, injectivity is checked against the row, the
 //     label/degree/neighbour-label filter prunes, and survivors are appended
 //     with warp-aggregated atomics (__ballot_sync / __popc);
 //   * a table chunk never holds more than `cap` rows: the host walks the
@@ -22,7 +23,9 @@
 //     descending, so intermediate results never exceed the scratch budget;
 //   * in count mode the last position is never materialised: when it has a
 //     single backward neighbour its count is the slice length minus the
-//     injectivity collisions, added while expanding the position before it.
+//     injectivity collisions, added while expanding the position before it;
+//     a two-position pendant tail is counted from two-hop aggregates while
+//     expanding the position three before the end.
 #include <algorithm>
 #include <cstring>
 #include <numeric>
@@ -61,6 +64,8 @@ struct Workspace {
   uint64_t* bsum = nullptr;
   uint32_t bsum_cap = 0;
   uint32_t* tile_row = nullptr;  // first row of every expand tile of a segment
+  uint32_t* root_keep = nullptr; // matrix-filter keep bits of the level-0 candidates
+  uint64_t root_keep_words = 0;
   TailStore tails;
   unsigned long long* ctr = nullptr;     // device counters
   unsigned long long* h_ctr = nullptr;   // pinned mirror
@@ -219,6 +224,8 @@ struct StepArgs {
   uint64_t seg_cap;              // elements one lane expand launch can tile
   unsigned long long* scan_status;  // look-back words of the work/scan kernel
   uint32_t spin_limit;           // bounded device waits (iterations)
+  const uint32_t* root_keep;     // level-0 candidates kept by the matrix filter
+                                 // (bit per vertex; nullptr: no filter)
 };
 
 // Rows of the input table of a lane launch at level a.level.
@@ -276,11 +283,13 @@ __device__ __forceinline__ bool in_slice_se(const GraphDev& g, uint32_t d, uint3
 // a hub needs no slice offsets at all.
 __device__ __forceinline__ bool in_slice(const GraphDev& g, uint32_t d, uint32_t y, uint32_t lab,
                                          uint32_t x, uint32_t pmin) {
+  uint32_t s, e;
   if (g.hub_slot[d] && pmin <= 1) {
     const uint16_t h = __ldg(g.hub_slot[d] + y);
     if (h != NO_HUB) return hub_bit(g, d, h, x);
+    slice_of(g, d, y, lab, s, e);  // not a hub: search the slice
+    return contains(g.adj[d], s, e, x);
   }
-  uint32_t s, e;
   slice_of(g, d, y, lab, s, e);
   return in_slice_se(g, d, y, s, e, x, pmin);
 }
@@ -663,6 +672,7 @@ enum : int {
   X_EMIT = 2,   // complete matches are written as rows (emit mode)
   X_FUSED = 4,  // the last position (one backward slice) is closed in place
   X_TAIL = 8,   // a two-position pendant tail is closed from dense aggregates
+  X_ONE = 16,   // one query, no row query ids: its plan is staged in shared memory
 };
 
 // Expand kernel: one element (row, driving entry) per thread.
@@ -686,6 +696,15 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
   // hub row's elements still spread over many blocks.
   __shared__ unsigned long long s_base, s_wbase;
   __shared__ uint32_t s_wcnt[EXPAND_BLOCK / 32];
+  // A single query's plan is read by every element: staged once per block,
+  // its fields are shared-memory loads with 32-bit addressing.
+  __shared__ PlanDev s_plan;
+  if constexpr ((MODE & X_ONE) != 0) {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(a.plans);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&s_plan);
+    for (uint32_t w = threadIdx.x; w < sizeof(PlanDev) / 4; w += EXPAND_BLOCK) dst[w] = src[w];
+    __syncthreads();
+  }
   // Tiles per grab: about 16 grabs per block over the launch (fewer queue
   // atomics and barriers), at least 4, at most 32.
   uint64_t grab = a.grab;
@@ -713,8 +732,14 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
         const uint32_t e = uint32_t(t - a.woff[r]);
         const uint8_t ci = a.dci[r];
         const uint32_t ds = a.dstart[r];
-        q = a.in.qid ? a.in.qid[r] : 0u;
-        const PlanDev& P = a.plans[q];
+        const PlanDev* Pp;
+        if constexpr ((MODE & X_ONE) != 0) {
+          Pp = &s_plan;
+        } else {
+          q = a.in.qid ? a.in.qid[r] : 0u;
+          Pp = a.plans + q;
+        }
+        const PlanDev& P = *Pp;
         const uint32_t lab = P.label[i];
         uint32_t ddir = 0;
         if (ci == DCI_BUCKET) {
@@ -724,6 +749,9 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
           x = __ldg(g.adj[ddir] + ds + e);
         }
         ok = true;
+        // the lossy matrix filter drops level-0 candidates it rejects
+        if (i == 0 && a.root_keep && !((__ldg(a.root_keep + (x >> 5)) >> (x & 31)) & 1u))
+          ok = false;
         // injectivity: only earlier positions with the same label can collide
         for (uint32_t m = P.samelab[i]; m && ok; m &= m - 1) {
           const uint32_t j = __ffs(m) - 1;
@@ -843,7 +871,7 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
         if (em) {
           const unsigned long long idx = base + __popc(emm & lanemask_lt());
           if (idx < a.emit_cap) {
-            const PlanDev& P = a.plans[q];
+            const PlanDev& P = (MODE & X_ONE) ? s_plan : a.plans[q];
             for (uint32_t j = 0; j < i; ++j)
               a.emit_col[P.perm[j]][idx] = __ldg(g.globalid + a.in.col[j][r]);
             a.emit_col[P.perm[i]][idx] = __ldg(g.globalid + x);
@@ -1169,8 +1197,9 @@ static void launch_expand(const StepArgs& a, const PlanDev* plans, uint32_t npla
     if (a.tail_dense && p.tail2 && p.k == i + 3) tail = true;
     if (!count_mode && p.k == i + 1) emit = true;
   }
+  const bool one = nplans == 1 && a.in.qid == nullptr;
   const int mode = (writes ? X_WRITE : 0) | (emit ? X_EMIT : 0) | (fused ? X_FUSED : 0) |
-                   (tail ? X_TAIL : 0);
+                   (tail ? X_TAIL : 0) | (one ? X_ONE : 0);
   switch (mode) {
 #define MG_X(m) \
   case m:       \
@@ -1178,6 +1207,8 @@ static void launch_expand(const StepArgs& a, const PlanDev* plans, uint32_t npla
     break;
     MG_X(0) MG_X(1) MG_X(2) MG_X(3) MG_X(4) MG_X(5) MG_X(6) MG_X(7)
     MG_X(8) MG_X(9) MG_X(10) MG_X(11) MG_X(12) MG_X(13) MG_X(14) MG_X(15)
+    MG_X(16) MG_X(17) MG_X(18) MG_X(19) MG_X(20) MG_X(21) MG_X(22) MG_X(23)
+    MG_X(24) MG_X(25) MG_X(26) MG_X(27) MG_X(28) MG_X(29) MG_X(30) MG_X(31)
 #undef MG_X
   }
 }
@@ -1305,6 +1336,18 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
   const bool batch = nq > 1;
   if (batch) {
     k_iota<<<grid_for(nq, 256, 1024), 256, 0, st>>>(ws->qid[0], nq);
+    res->launches++;
+  }
+  if (o.matrix_filter && !batch && !plans[0].zero) {
+    const uint64_t words = (uint64_t(dg->g.n) + 31) / 32;
+    if (ws->root_keep_words < words) {
+      if ((rc = ws_alloc(ws, (void**)&ws->root_keep, words * 4))) return rc;
+      ws->root_keep_words = words;
+    }
+    if ((rc = matrix_filter_roots(o.matrix_filter, dg, plans[0].perm[0], plans[0].label[0],
+                                  ws->root_keep, st)))
+      return rc;
+    a.root_keep = ws->root_keep;
     res->launches++;
   }
   uint64_t T[MAXK] = {}, cur[MAXK] = {};
@@ -1595,15 +1638,6 @@ static int sort_and_copy(DevGraph* dg, const EmitBuf& eb, uint32_t k, uint64_t n
 // ---------------------------------------------------------------------------
 // Entry-point bodies
 // ---------------------------------------------------------------------------
-struct DeviceGuard {
-  int prev = 0;
-  explicit DeviceGuard(int d) {
-    cudaGetDevice(&prev);
-    cudaSetDevice(d);
-  }
-  ~DeviceGuard() { cudaSetDevice(prev); }
-};
-
 static mg_opts resolve_opts(const mg_opts* o) {
   mg_opts r;
   mg_opts_default(&r);
@@ -2045,6 +2079,8 @@ int subiso_batch(DevGraph* dg, const mg_csr_view* const* qs, uint32_t nq, const 
                  uint64_t* counts, mg_stats* st, const uint32_t* orders = nullptr,
                  uint64_t* level_rows = nullptr) {
   const mg_opts o = resolve_opts(opts);
+  if (o.matrix_filter)
+    return set_error(MG_E_ARG, "matrix_filter applies to single-query count and emit only");
   std::vector<PlanDev> plans(nq);
   std::vector<uint32_t> learned;
   if (!orders && o.order == MG_ORDER_LEARNED && o.model) {
@@ -2333,6 +2369,8 @@ int noalloc_count(DevGraph* dg, const mg_csr_view* q, const mg_opts* opts, uint6
   // Every argument is checked before any work is queued on the shared array.
   int rc = check_opts(o);
   if (rc) return rc;
+  if (o.matrix_filter)
+    return set_error(MG_E_ARG, "mg_subiso_count_noalloc does not apply a matrix filter");
   QueryGraph Q;
   rc = normalise_query(q, &Q);  // the allocating entry points' normaliser
   if (rc) return rc;

@@ -13,13 +13,15 @@ void Check(int rc) {
 
 SubIso::SubIso(const std::string& pattern_path, const std::string& data_graph_path,
                const std::string& data_graph_edgelist_path, const std::string& output_path,
-               const std::string& mode, int order, int device, const std::string& model_path)
+               const std::string& mode, int order, int device, const std::string& model_path,
+               const std::vector<std::string>& matrix_paths)
     : pattern_path_(pattern_path),
       data_graph_path_(data_graph_path),
       data_graph_edgelist_path_(data_graph_edgelist_path),
       output_path_(output_path),
       mode_(mode),
       model_path_(model_path),
+      matrix_paths_(matrix_paths),
       order_(order),
       device_(device) {}
 
@@ -41,17 +43,30 @@ void SubIso::Run() {
   void* model = nullptr;
   if (order_ == MG_ORDER_LEARNED && !model_path_.empty())
     Check(mg_order_model_load(model_path_.c_str(), device_, &model));
+  void* filter = nullptr;
+  if (matrix_paths_.size() == 6) {
+    const char* dirs[6];
+    for (int i = 0; i < 6; ++i) dirs[i] = matrix_paths_[i].c_str();
+    int frc = mg_matrix_filter_load(dirs, device_, &filter);
+    if (frc != MG_OK) {
+      const std::string msg = mg_last_error();
+      if (model) mg_order_model_free(model);
+      throw Error(frc, msg);
+    }
+  }
   void* dg = nullptr;
   int rc = mg_graph_upload(&g_, device_, &dg);
   if (rc != MG_OK) {
     const std::string msg = mg_last_error();
     if (model) mg_order_model_free(model);
+    if (filter) mg_matrix_filter_free(filter);
     throw Error(rc, msg);
   }
   mg_opts o;
   mg_opts_default(&o);
   o.order = order_;
   o.model = model;
+  o.matrix_filter = filter;
   mg_stats st;
   rc = mg_subiso_count_ex(dg, &p_, &o, &count_, &st);
   if (rc == MG_OK && mode_ == "emit") {
@@ -64,6 +79,7 @@ void SubIso::Run() {
   const std::string msg = rc == MG_OK ? "" : mg_last_error();
   mg_graph_free(dg);
   if (model) mg_order_model_free(model);
+  if (filter) mg_matrix_filter_free(filter);
   if (rc != MG_OK) throw Error(rc, msg);
   match_ms_ = st.device_ms;
   std::cout << "[SubIso] LoadData() elapsed: "

@@ -39,10 +39,14 @@ void Check(int rc);
 
 class SubIso {
  public:
+  // matrix_paths: the six directories of the reference CPUSubIso's
+  // matrix_path1..6 (core/task/cpu_task/cpu_subiso.cuh:32-39); all six set
+  // turn on the lossy MatrixFilter on the level-0 candidates.
   SubIso(const std::string& pattern_path, const std::string& data_graph_path,
          const std::string& data_graph_edgelist_path, const std::string& output_path,
          const std::string& mode = "count", int order = MG_ORDER_REFERENCE, int device = 0,
-         const std::string& model_path = "");
+         const std::string& model_path = "",
+         const std::vector<std::string>& matrix_paths = {});
   ~SubIso();
   void Run();
 
@@ -56,6 +60,7 @@ class SubIso {
 
   std::string pattern_path_, data_graph_path_, data_graph_edgelist_path_, output_path_;
   std::string mode_, model_path_;
+  std::vector<std::string> matrix_paths_;
   int order_, device_;
   mg_csr_view p_{}, g_{};
   void* p_owner_ = nullptr;

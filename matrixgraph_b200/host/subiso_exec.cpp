@@ -3,9 +3,13 @@
 // [-o <output>] [-scheduler CHBL|EvenSplit|RoundRobin] plus
 // [-mode count|emit] [-order reference|heuristic|strong|learned]
 // [-model <order model dir/>] [-batch <file of pattern dirs, one per line>]
-// [-device N] [-tune <autotuner table>].  With -batch, -p is not needed and
-// every pattern is counted in batched calls (one per tuned query-size bucket
-// with -tune); -o receives "pattern count" lines.
+// [-device N] [-tune <autotuner table>] [-m1 .. -m6 <matrix dir/>].  With
+// -batch, -p is not needed and every pattern is counted in batched calls (one
+// per tuned query-size bucket with -tune); -o receives "pattern count" lines.
+// -m1..-m6 are the six matrices of the reference CPU subiso's MatrixFilter
+// (apps/cpu_subiso.cpp, core/task/cpu_task/cpu_subiso.cuh:32-39): all six
+// turn on the lossy learned filter of the level-0 candidates (single
+// pattern only).
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
@@ -30,7 +34,8 @@ int main(int argc, char** argv) {
   std::map<std::string, std::string> flags = {
       {"p", ""}, {"g", ""}, {"e", ""}, {"o", ""}, {"scheduler", "CHBL"},
       {"mode", "count"}, {"order", "reference"}, {"device", "0"}, {"batch", ""},
-      {"model", ""}, {"tune", ""}};
+      {"model", ""}, {"tune", ""}, {"m1", ""}, {"m2", ""}, {"m3", ""}, {"m4", ""},
+      {"m5", ""}, {"m6", ""}};
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i];
     while (!a.empty() && a[0] == '-') a = a.substr(1);
@@ -85,11 +90,22 @@ int main(int argc, char** argv) {
     std::cerr << "Error: Data graph path (-g) is required" << std::endl;
     ok = false;
   }
+  std::vector<std::string> matrix_paths;
+  for (const char* m : {"m1", "m2", "m3", "m4", "m5", "m6"})
+    if (!flags[m].empty()) matrix_paths.push_back(flags[m]);
+  if (!matrix_paths.empty() && matrix_paths.size() != 6) {
+    std::cerr << "Error: the matrix filter needs all of -m1 .. -m6" << std::endl;
+    ok = false;
+  }
+  if (!matrix_paths.empty() && !batch.empty()) {
+    std::cerr << "Error: -m1 .. -m6 apply to a single pattern (-p), not to -batch" << std::endl;
+    ok = false;
+  }
   if (!ok) {
     std::cerr << "Usage: " << argv[0] << " -p <pattern_path/> -g <graph_path/> [-e <edge_list>]"
               << " [-o <output_path>] [-scheduler CHBL] [-mode count|emit]"
               << " [-order reference|strong|learned] [-model <dir/>] [-batch <list>]"
-              << " [-device N] [-tune <table>]" << std::endl;
+              << " [-device N] [-tune <table>] [-m1 .. -m6 <matrix dir/>]" << std::endl;
     return EXIT_FAILURE;
   }
   std::cout << "\n=== SubIso Configuration ===\nPattern Graph: " << flags["p"]
@@ -106,7 +122,7 @@ int main(int argc, char** argv) {
       system.Run(matrixgraph::kSubIso, &task);
     } else {
       SubIso task(flags["p"], flags["g"], flags["e"], flags["o"], flags["mode"], order, device,
-                  flags["model"]);
+                  flags["model"], matrix_paths);
       system.Run(matrixgraph::kSubIso, &task);
     }
   } catch (const std::exception& e) {

@@ -33,7 +33,8 @@ ORDERS = {"reference": L.MG_ORDER_REFERENCE, "heuristic": L.MG_ORDER_REFERENCE,
 
 def make_opts(order="reference", filters=L.MG_FILTER_ALL, chunk_rows=0, given_order=None,
               model=None, root_range=None, mem_budget_bytes=0, root_step=0,
-              grab=0, no_tail=0, max_elements=0, probe_min=0, kernel_events=0, lanes=0):
+              grab=0, no_tail=0, max_elements=0, probe_min=0, kernel_events=0, lanes=0,
+              matrix_filter=None):
     o = L.default_opts()
     o.no_tail = no_tail
     o.max_elements = max_elements
@@ -53,6 +54,9 @@ def make_opts(order="reference", filters=L.MG_FILTER_ALL, chunk_rows=0, given_or
         o.order = L.MG_ORDER_GIVEN
     if model is not None:
         o.model = model.handle if hasattr(model, "handle") else model
+    if matrix_filter is not None:
+        o.matrix_filter = (matrix_filter.handle if hasattr(matrix_filter, "handle")
+                           else matrix_filter)
     if root_range is not None:
         o.root_begin, o.root_end = int(root_range[0]), int(root_range[1])
     return o, keep
@@ -229,12 +233,15 @@ class SchedulerType(enum.IntEnum):
 
 
 class SubIso:
-    """``SubIso`` task: pattern and data graph CSR directories in, exact matches out."""
+    """``SubIso`` task: pattern and data graph CSR directories in, exact matches
+    out.  ``matrix_paths``: the six matrix directories of the reference's
+    CPUSubIso (matrix_path1..6, core/task/cpu_task/cpu_subiso.cuh:32-39);
+    when given, the lossy MatrixFilter drops level-0 candidates."""
 
     def __init__(self, pattern_path: str, data_graph_path: str,
                  data_graph_edgelist_path: str = "", output_path: str = "",
                  mode: str = "count", order: str = "reference", device: int = 0,
-                 model=None):
+                 model=None, matrix_paths=None):
         self.pattern_path = pattern_path
         self.data_graph_path = data_graph_path
         self.data_graph_edgelist_path = data_graph_edgelist_path  # unused, as in the reference
@@ -243,6 +250,7 @@ class SubIso:
         self.order = order
         self.device = device
         self.model = model
+        self.matrix_paths = list(matrix_paths) if matrix_paths else None
         self.count = None
         self.rows = None
         self.timings = {}
@@ -256,13 +264,20 @@ class SubIso:
         self.LoadData()
         t1 = time.perf_counter()
         dg = DeviceGraph(self.g_, self.device)
+        mf = None
         try:
+            if self.matrix_paths:
+                from .matrix_filter import MatrixFilter
+                mf = MatrixFilter.load(self.matrix_paths, self.device)
             t2 = time.perf_counter()
-            self.count = dg.count(self.p_, order=self.order, model=self.model)
+            kw = {"order": self.order, "model": self.model, "matrix_filter": mf}
+            self.count = dg.count(self.p_, **kw)
             if self.mode == "emit":
-                self.rows = dg.emit(self.p_, cap=self.count, order=self.order, model=self.model)
+                self.rows = dg.emit(self.p_, cap=self.count, **kw)
             t3 = time.perf_counter()
         finally:
+            if mf is not None:
+                mf.free()
             dg.free()
         self.timings = {"load_s": t1 - t0, "upload_s": t2 - t1, "match_s": t3 - t2}
         if self.output_path:
