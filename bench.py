@@ -249,7 +249,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": "exact embeddings/s", "value": value,
             "unit": "embeddings/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "scaling": "strong", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": config(args.scale, g.n, g.m, args.queries),
             "cpu_baseline": {"value": value, "unit": "embeddings/s", "cores": threads,
                              "kind": "port", "sample": sample},
@@ -302,14 +302,17 @@ def same_work(dg, qs, names, cpu_rows, device, e2e_graph):
             "speedup_e2e": cpu_s / e2e_s if e2e_s > 0 else None}
 
 
-def c3_oracle_sample(g, og, every=64, max_elements=10 ** 7):
+def c3_oracle_sample(g, og, every=32, max_elements=10 ** 7, max_count=10 ** 8):
     """Oracle counts of a systematic sample of the 4,096-query batch: every
     `every`-th query among those whose reference order expands at most
-    `max_elements` candidates.  Returns {index: count}."""
+    `max_elements` candidates and whose recorded count is at most `max_count`
+    (the oracle enumerates every match, so the count bounds its time).
+    Returns {index: count}."""
     import oracle as O
     from matrixgraph_b200 import workloads as W
     qs, rec = W.batch_queries(g)
-    picked = [i for i in range(0, len(qs), every) if rec["elements"][i] <= max_elements]
+    picked = [i for i in range(0, len(qs), every)
+              if rec["elements"][i] <= max_elements and rec["counts"][i] <= max_count]
     threads = os.cpu_count() or 1
     return {i: O.count(og, O.query_from_csr(qs[i]), threads=threads)["count"] for i in picked}
 
@@ -490,76 +493,30 @@ def c5_workload(n_queries):
     return out
 
 
-def heldout_eval(dg, g, n=512, budget=1 << 28):
-    """Learned vs reference order on held-out queries (configuration C4):
-    seeds 200000 .. 200000+n-1 taken in order — the selection depends on
-    neither order — random connected, k uniform 6-10, walk labels, on the
-    resident scale-22 graph.  The orders of the whole set are planned in one
-    call each (the learned one through one inference launch; its time is the
-    planning cost), and every query is counted under both orders with the
-    same element budget.  A query past the budget under an order is censored
-    there: a censored reference against a finished learned order counts as a
-    win, the reverse as a loss, and queries censored under both are left out
-    of the medians.  Counts under both orders must be equal."""
-    import numpy as np
-
-    from matrixgraph_b200 import _lib as L
+def heldout_eval(dg, g, n=512):
+    """Learned vs reference order on held-out queries (configuration C4): the
+    first n queries of the committed held-out test set
+    (matrixgraph_b200/data/heldout_seeds.json: random connected, k 6-10, walk
+    labels, seeds from 200000 kept when one of three seeded random orders
+    counts them within 2^24 candidate elements — a criterion that depends on
+    neither order under test; even positions are the test set, odd ones
+    chose the model) on the resident scale-22 graph, each counted under both
+    orders with the same element budget; counts must equal the recorded
+    ones."""
     from matrixgraph_b200 import workloads as W
     from matrixgraph_b200.order_model import OrderModel
+    with open(W.HELDOUT_SEEDS) as f:
+        rec = json.load(f)
+    test, _ = W.heldout_split(rec)
     model = OrderModel.load(W.MODEL_DIR)
-    qs = [W.learned_query(g, W.EVAL_FIRST_SEED + i) for i in range(n)]
-    ref_orders = dg.plan_orders(qs, order="reference")
-    t0 = time.perf_counter()
-    learned_orders = dg.plan_orders(qs, order="learned", model=model)
-    plan_s = time.perf_counter() - t0
+    summary, _ = W.compare_orders(dg, g, test[:n], model)
     model.free()
-    res = []
-    for q, ro, lo in zip(qs, ref_orders, learned_orders):
-        r = {}
-        for name, od in (("ref", ro), ("learned", lo)):
-            try:
-                c, st = dg.count(q, stats=True, given_order=od, max_elements=budget)
-                r[name] = (c, st["device_ms"], st["elements"])
-            except L.MGError as e:
-                if e.code != L.MG_E_LIMIT:
-                    raise
-                r[name] = None
-        if r["ref"] and r["learned"]:
-            assert r["ref"][0] == r["learned"][0], "counts differ between orders"
-        res.append(r)
-    plan_ms = 1e3 * plan_s / n
-    sp, sp_plan, el, sp_both = [], [], [], []
-    both = ref_only = learned_only = neither = 0
-    for r in res:
-        a, b = r["ref"], r["learned"]
-        if a and b:
-            both += 1
-            sp.append(a[1] / b[1])
-            sp_both.append(a[1] / b[1])
-            sp_plan.append(a[1] / (b[1] + plan_ms))
-            el.append(a[2] / max(1, b[2]))
-        elif b:
-            learned_only += 1
-            sp.append(float("inf"))
-            sp_plan.append(float("inf"))
-        elif a:
-            ref_only += 1
-            sp.append(0.0)
-            sp_plan.append(0.0)
-        else:
-            neither += 1
-    med = float(np.median(sp)) if sp else None
-    return {"workload": f"{n} held-out random connected queries (seeds 200000..{200000 + n - 1}, "
-                        "k 6-10, p_extra 0.3, walk labels) on the R-MAT scale-22 graph; budget "
-                        f"{budget} candidate elements per count",
-            "model": "matrixgraph_b200/data/order_model", "n": n,
-            "finished_both": both, "finished_learned_only": learned_only,
-            "finished_reference_only": ref_only, "finished_neither": neither,
-            "median_speedup_device": med,
-            "median_speedup_with_planning": float(np.median(sp_plan)) if sp_plan else None,
-            "median_speedup_device_both_finished": float(np.median(sp_both)) if sp_both else None,
-            "median_element_ratio_both_finished": float(np.median(el)) if el else None,
-            "planning_ms_per_query": plan_ms}
+    summary["workload"] = (f"{min(n, len(test))} held-out queries of "
+                           "matrixgraph_b200/data/heldout_seeds.json (test half; k 6-10, "
+                           "p_extra 0.3, walk labels) on the R-MAT scale-22 graph; budget "
+                           f"{summary['budget_elements']} candidate elements per count")
+    summary["model"] = "matrixgraph_b200/data/order_model"
+    return summary
 
 
 def run_mine(args):
@@ -717,7 +674,7 @@ def run_mine(args):
     if rank == 0:
         line = {"metric": "exact embeddings/s", "value": value, "unit": "embeddings/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
                 "vs_baseline": None, "dtype": "u32", "data": "synthetic",
                 "config": config(args.scale, g.n, g.m_out, args.queries),
                 "queries_per_s": len(qs) / (ms_step / 1e3),

@@ -352,25 +352,6 @@ int  mg_order_model_features(void* dgraph, const mg_csr_view* q, float* x, float
 int  mg_selftest_wait_timeout(void* dgraph, const mg_csr_view* q, uint32_t spin_limit,
                               int* status);
 
-/* Exact count that allocates nothing.  No counterpart in the reference.
- *
- * For callers that cannot allocate device memory when they ask for a count:
- * processes whose HBM is owned by another allocator (a framework's caching
- * allocator or a fixed arena that has reserved nearly all of it), and
- * latency-critical paths that must not pay for cudaMalloc/cudaFree or the
- * device-wide synchronisation cudaFree implies.  The enumeration scratch
- * (level tables, scan space, counters, plan) lives in one file-scope device
- * array of MG_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
- * until the process exits; the level tables are sized to fit it, so any
- * match count is reachable (more, smaller chunks).  A caller-set chunk_rows
- * whose tables do not fit is rejected with MG_E_LIMIT.  The data graph must
- * already be resident (mg_graph_upload); orders: reference, strong, given.
- * The first call on a device looks up the array's device address with that
- * device current; make that first call before any stream capture.  Every
- * call shares the array and leaves its contents behind (counters are
- * cleared at the start of each call); calls are serialised by a process-wide
- * lock, since calls that overlapped on the GPU would race on the array.    */
-#define MG_NOALLOC_SCRATCH_BYTES (16u << 20)
 /* ---- lossy learned candidate filter (MatrixFilter) ---------------------
  * Replaces the reference's MatrixFilter (core/task/cpu_task/cpu_subiso.cu:
  * 237-277) with its CPU MLP helpers (core/task/gpu_task/kernel/
@@ -393,6 +374,25 @@ void mg_matrix_filter_free(void* filter);
 int  mg_matrix_filter_keep(void* filter, uint32_t u, const uint32_t* v, uint64_t nv,
                            uint8_t* keep);
 
+/* Exact count that allocates nothing.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory when they ask for a count:
+ * processes whose HBM is owned by another allocator (a framework's caching
+ * allocator or a fixed arena that has reserved nearly all of it), and
+ * latency-critical paths that must not pay for cudaMalloc/cudaFree or the
+ * device-wide synchronisation cudaFree implies.  The enumeration scratch
+ * (level tables, scan space, counters, plan) lives in one file-scope device
+ * array of MG_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
+ * until the process exits; the level tables are sized to fit it, so any
+ * match count is reachable (more, smaller chunks).  A caller-set chunk_rows
+ * whose tables do not fit is rejected with MG_E_LIMIT.  The data graph must
+ * already be resident (mg_graph_upload); orders: reference, strong, given.
+ * The first call on a device looks up the array's device address with that
+ * device current; make that first call before any stream capture.  Every
+ * call shares the array and leaves its contents behind (counters are
+ * cleared at the start of each call); calls are serialised by a process-wide
+ * lock, since calls that overlapped on the GPU would race on the array.    */
+#define MG_NOALLOC_SCRATCH_BYTES (16u << 20)
 int  mg_subiso_count_noalloc(void* dgraph, const mg_csr_view* q, const mg_opts* opts,
                              uint64_t* count);
 

@@ -1990,7 +1990,16 @@ static int subiso_batch_lanes(DevGraph* dg, std::vector<PlanDev>& plans, const m
       std::vector<uint64_t> l1(MAXK + 1, 0);
       mg_opts o1 = o;
       o1.chunk_rows = 0;
-      if ((rc = run_levels(dg, one, true, nullptr, o1, &c1, &r1, l1.data()))) return rc;
+      rc = run_levels(dg, one, true, nullptr, o1, &c1, &r1, l1.data());
+      if (rc == MG_E_LIMIT && o.max_elements) {
+        // Past the per-query budget on the chunked path as well: unknown, as a
+        // query over budget in its lane reports.
+        cnt[j] = ~0ull;
+        for (uint32_t i = 0; i <= MAXK; ++i) lv[uint64_t(j) * (MAXK + 1) + i] = 0;
+        res->reruns++;
+        continue;
+      }
+      if (rc) return rc;
       cnt[j] = c1;
       for (uint32_t i = 0; i <= MAXK; ++i) lv[uint64_t(j) * (MAXK + 1) + i] = l1[i];
       res->balg += r1.balg;

@@ -198,6 +198,51 @@ def shard_roots(n_roots: int, rank: int, world: int) -> tuple[int, int]:
     return begin, begin + base + (1 if rank < rem else 0)
 
 
+def root_costs(g: CSRGraph, q: CSRGraph, order="reference") -> np.ndarray:
+    """Estimated cost of each level-0 candidate of a query, in bucket order:
+    its degree (the length of the lists its subtree starts from).  The bucket
+    of the first vertex of the order lists that label's vertices by
+    ascending id, as the engine's label bucket does."""
+    lab = g.array("labels")
+    first = plan_order(q, order=order)[0]
+    bucket = np.flatnonzero(lab == q.array("labels")[first])
+    return np.diff(g.array("out_off").astype(np.int64))[bucket]
+
+
+def shard_roots_weighted(costs, rank: int, world: int) -> tuple[int, int]:
+    """Contiguous level-0 range of one rank cut from the prefix sum of the
+    candidates' estimated costs: rank r takes the candidates whose cost
+    prefix falls in [r/world, (r+1)/world) of the total, so a bucket whose
+    head holds the hubs is not handed to rank 0 whole.  The ranges of all
+    ranks partition the bucket."""
+    c = np.asarray(costs, dtype=np.float64)
+    n = len(c)
+    if world <= 1 or n == 0:
+        return (0, n) if rank == 0 or world <= 1 else (n, n)
+    tot = c.sum()
+    if tot <= 0:
+        return shard_roots(n, rank, world)
+    mid = np.cumsum(c) - 0.5 * c  # cost midpoint of each candidate
+    cut = lambda r: int(np.searchsorted(mid, tot * r / world, side="left"))  # noqa: E731
+    return cut(rank), cut(rank + 1) if rank + 1 < world else n
+
+
+def shard_batch(costs, rank: int, world: int) -> list[int]:
+    """Query indices of one rank's share of a batch: queries in decreasing
+    estimated cost, each to the rank with the least cost so far (ties to the
+    lower rank).  Deterministic, so every rank computes the same split
+    without an exchange; the shares partition the batch."""
+    c = np.asarray(costs, dtype=np.float64)
+    load = np.zeros(max(1, world))
+    mine = []
+    for i in sorted(range(len(c)), key=lambda j: (-c[j], j)):
+        r = int(np.argmin(load))
+        load[r] += c[i]
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
+
+
 def shard_strided(rank: int, world: int) -> dict:
     """Count options of one rank's shard: level-0 candidates at bucket
     positions rank, rank + world, rank + 2*world, ...  A label bucket lists

@@ -18,7 +18,7 @@
 
     python -m matrixgraph_b200.workloads select-batch OUT.json
     python -m matrixgraph_b200.workloads train-order OUTDIR [N]
-    python -m matrixgraph_b200.workloads eval-order MODEL_DIR/ OUT.json [N]
+    python -m matrixgraph_b200.workloads c4 OUTDIR [N_TRAIN]
     python -m matrixgraph_b200.workloads eval-batch MODEL_DIR/ OUT.json
 
 Learned order: training queries are random connected queries with k uniform
@@ -222,63 +222,184 @@ def train_order(outdir: str, n_train: int = 8000, n_random: int = 8, epochs: int
     return rec
 
 
-def eval_order(model_dir: str, out_path: str, n_eval: int = 2000, log=print,
-               select_seconds: float = 150.0):
-    """Held-out queries (k 6..10) on the scale-22 graph: reference vs learned."""
+HELDOUT_SEEDS = os.path.join(HERE, "data", "heldout_seeds.json")
+SELECT_BUDGET = 1 << 24
+SELECT_ORDERS = 3
+
+
+def selection_orders(q, seed: int):
+    """SELECT_ORDERS random connected orders of a query, seeded by the query's
+    own seed only: they depend on neither the reference nor a learned order."""
+    from .order_model import random_connected_order
+    rng = np.random.default_rng([seed, 0x5E1EC7])
+    return [random_connected_order(q, rng) for _ in range(SELECT_ORDERS)]
+
+
+def select_heldout(dg: DeviceGraph, g, first_seed: int = EVAL_FIRST_SEED,
+                   budget: int = SELECT_BUDGET, max_seeds: int = 1 << 17,
+                   max_seconds: float | None = None, chunk: int = 1024, log=None):
+    """Held-out queries (k 6..10, seeds from first_seed, taken in order) that
+    some order can count: a seed is kept when at least one of its
+    SELECT_ORDERS seeded random connected orders finishes within `budget`
+    candidate elements.  The criterion depends on neither order under test;
+    element counts are exact, so for a given number of scanned seeds the
+    selection is deterministic.  Every finished order of a query must give the
+    same count, which is recorded."""
+    import time
+    from .order_model import UNKNOWN
+    t0 = time.time()
+    kept, s = [], first_seed
+    while s - first_seed < max_seeds:
+        if max_seconds and time.time() - t0 > max_seconds:
+            break
+        seeds = list(range(s, s + chunk))
+        qs = [learned_query(g, x) for x in seeds]
+        jobs = [(i, o) for i, q in enumerate(qs) for o in selection_orders(q, seeds[i])]
+        counts, rows, _ = dg.batch_count_orders([qs[i] for i, _ in jobs], [o for _, o in jobs],
+                                                max_elements=budget)
+        for i, q in enumerate(qs):
+            fin = [j for j in range(i * SELECT_ORDERS, (i + 1) * SELECT_ORDERS)
+                   if counts[j] != UNKNOWN]
+            if not fin:
+                continue
+            cs = {int(counts[j]) for j in fin}
+            assert len(cs) == 1, (seeds[i], cs)
+            work = min(int(rows[j][1:q.n].sum()) for j in fin)
+            kept.append({"seed": seeds[i], "k": q.n, "count": cs.pop(), "best_random_prefixes": work})
+        s += chunk
+        if log:
+            log(f"scanned {s - first_seed} seeds, kept {len(kept)} ({time.time() - t0:.0f} s)")
+    return {"graph": "rmat scale 22 (workloads.rmat_graph)", "first_seed": first_seed,
+            "seeds_scanned": s - first_seed, "budget_elements": budget,
+            "orders_per_seed": SELECT_ORDERS,
+            "criterion": "some seeded random connected order finishes within the budget",
+            "queries": kept}
+
+
+def heldout_split(rec):
+    """Kept queries alternate between the held-out test set (even positions)
+    and the validation set used for model selection (odd positions)."""
+    qs = rec["queries"]
+    return qs[0::2], qs[1::2]
+
+
+def compare_orders(dg: DeviceGraph, g, recs, model, budget: int = EVAL_BUDGET):
+    """Learned against reference order on the queries of `recs` (selection
+    records with seed and count): both orders planned for the whole set in one
+    call each (the learned one through one inference launch: its time is the
+    planning cost), every query counted under both with the same element
+    budget, and counts checked against the recorded ones.  An order past the
+    budget is censored: a censored reference against a finished learned order
+    is a win, the reverse a loss, and queries censored under both are left out of the medians.  A censored run
+    reports no time, so its time is estimated as the budget at the finished
+    order's measured elements per ms."""
+    import time
+    qs = [learned_query(g, r["seed"]) for r in recs]
+    ref_orders = dg.plan_orders(qs, order="reference")
+    t0 = time.perf_counter()
+    lrn_orders = dg.plan_orders(qs, order="learned", model=model)
+    plan_ms = 1e3 * (time.perf_counter() - t0) / max(1, len(qs))
+    rows = []
+    for r, q, ro, lo in zip(recs, qs, ref_orders, lrn_orders):
+        row = {"seed": r["seed"], "k": q.n, "count": r["count"], "order_ref": ro,
+               "order_learned": lo}
+        for name, od in (("ref", ro), ("learned", lo)):
+            try:
+                c, st = dg.count(q, stats=True, given_order=od, max_elements=budget)
+                assert c == r["count"], (r["seed"], name, c, r["count"])
+                row[f"ms_{name}"] = st["device_ms"]
+                row[f"elements_{name}"] = st["elements"]
+                row[f"done_{name}"] = True
+            except L.MGError as e:
+                if e.code != L.MG_E_LIMIT:
+                    raise
+                row[f"ms_{name}"] = None
+                row[f"done_{name}"] = False
+        rows.append(row)
+    # A censored run reports no time, so a censored order is charged the
+    # budget at the finished order's measured elements per ms.
+    sp, sp_plan, el = [], [], []
+    n_both = n_lrn = n_ref = n_none = 0
+    for row in rows:
+        a, b = row["done_ref"], row["done_learned"]
+        if a and b:
+            n_both += 1
+            sp.append(row["ms_ref"] / row["ms_learned"])
+            sp_plan.append(row["ms_ref"] / (row["ms_learned"] + plan_ms))
+            el.append(row["elements_ref"] / max(1, row["elements_learned"]))
+        elif b:
+            n_lrn += 1
+            rate = row["elements_learned"] / max(row["ms_learned"], 1e-6)
+            lb = budget / rate
+            sp.append(lb / row["ms_learned"])
+            sp_plan.append(lb / (row["ms_learned"] + plan_ms))
+        elif a:
+            n_ref += 1
+            rate = row["elements_ref"] / max(row["ms_ref"], 1e-6)
+            ub = budget / rate
+            sp.append(row["ms_ref"] / ub)
+            sp_plan.append(row["ms_ref"] / (ub + plan_ms))
+        else:
+            n_none += 1
+    med = lambda v: float(np.median(v)) if v else None  # noqa: E731
+    geo = lambda v: float(np.exp(np.mean(np.log(v)))) if v else None  # noqa: E731
+    summary = {"n": len(rows), "budget_elements": budget, "finished_both": n_both,
+               "finished_learned_only": n_lrn, "finished_reference_only": n_ref,
+               "finished_neither": n_none,
+               "median_speedup_device": med(sp),
+               "median_speedup_with_planning": med(sp_plan),
+               "geomean_speedup_device": geo(sp),
+               "median_speedup_device_both_finished": med(
+                   [row["ms_ref"] / row["ms_learned"] for row in rows
+                    if row["done_ref"] and row["done_learned"]]),
+               "median_element_ratio_both_finished": med(el),
+               "planning_ms_per_query": plan_ms,
+               "censoring": "an order past the budget is charged the budget at the other "
+                            "order's measured elements per ms (an estimate, not a time)"}
+    return summary, rows
+
+
+def c4_pipeline(outdir: str, n_train: int = 6000, select_seconds: float = 300.0, log=print):
+    """Configuration C4 end to end on one GPU: held-out selection on the
+    scale-22 graph, training of a new network on the scale-20 graph, model
+    selection between the committed and the new network on the validation
+    half (median device speed-up), and the held-out test comparison of the
+    chosen one.  Writes heldout_seeds.json, order_model_new/,
+    order_train_record_new.json and order_eval.json into outdir."""
     import time
     from .order_model import OrderModel
     t0 = time.time()
     g = rmat_graph(22)
     dg = DeviceGraph(g)
-    model = OrderModel.load(model_dir)
-    kept, dropped = select_queries(dg, g, learned_query, EVAL_FIRST_SEED, n_eval, EVAL_BUDGET,
-                                   12 * n_eval, log, max_seconds=select_seconds)
-    log(f"held-out: kept {len(kept)} dropped {dropped} ({time.time() - t0:.1f}s)")
-    rows = []
-    for r in kept:
-        q = learned_query(g, r["seed"])
-        c_ref, st_ref = dg.count(q, stats=True)
-        t_plan = time.perf_counter()
-        lo = dg.plan_order(q, order="learned", model=model)
-        t_plan = time.perf_counter() - t_plan
-        guard = max(16 * r["elements"], 1 << 24)
-        try:
-            c_l, st_l = dg.count(q, stats=True, given_order=lo, max_elements=guard)
-            ms_l = st_l["device_ms"]
-            assert c_l == c_ref, (r["seed"], c_l, c_ref)
-        except L.MGError as e:
-            if e.code != L.MG_E_LIMIT:
-                raise
-            ms_l, st_l = float("inf"), None
-        try:
-            _, st_s = dg.count(q, stats=True, order="strong", max_elements=guard)
-            ms_s = st_s["device_ms"]
-        except L.MGError as e:
-            if e.code != L.MG_E_LIMIT:
-                raise
-            ms_s = float("inf")
-        rows.append({"seed": r["seed"], "k": q.n, "count": int(c_ref),
-                     "ms_ref": st_ref["device_ms"], "ms_learned": ms_l, "ms_strong": ms_s,
-                     "plan_ms": 1e3 * t_plan, "order_ref": st_ref["order"],
-                     "order_learned": lo, "rows_ref": st_ref["level_rows"],
-                     "rows_learned": st_l["level_rows"] if st_l else None})
-    sp = np.array([x["ms_ref"] / x["ms_learned"] for x in rows])
-    sp_wall = np.array([x["ms_ref"] / (x["ms_learned"] + x["plan_ms"]) for x in rows])
-    best = np.array([min(x["ms_ref"], x["ms_strong"], x["ms_learned"]) for x in rows])
-    regret = np.array([x["ms_learned"] / b for x, b in zip(rows, best)])
-    summary = {"n": len(rows), "dropped": dropped, "budget": EVAL_BUDGET,
-               "median_speedup_device": float(np.median(sp)) if len(sp) else None,
-               "median_speedup_with_planning": float(np.median(sp_wall)) if len(sp) else None,
-               "geomean_speedup_device": float(np.exp(np.mean(np.log(sp)))) if len(sp) else None,
-               "total_ms_ref": float(sum(x["ms_ref"] for x in rows)),
-               "total_ms_learned": float(sum(x["ms_learned"] for x in rows)),
-               "total_ms_strong": float(sum(x["ms_strong"] for x in rows)),
-               "median_regret": float(np.median(regret)) if len(sp) else None,
-               "learned_over_budget": int(sum(1 for x in rows if x["ms_learned"] == float("inf"))),
-               "seconds": time.time() - t0}
-    log(json.dumps(summary))
-    with open(out_path, "w") as f:
+    rec = select_heldout(dg, g, max_seconds=select_seconds, log=log)
+    with open(os.path.join(outdir, "heldout_seeds.json"), "w") as f:
+        json.dump(rec, f)
+    test, val = heldout_split(rec)
+    log(f"held-out: {len(rec['queries'])} kept of {rec['seeds_scanned']} "
+        f"({time.time() - t0:.0f} s)")
+    dg.free()
+    tr = train_order(os.path.join(outdir, "new"), n_train=n_train, log=log)
+    log(f"trained ({time.time() - t0:.0f} s): {json.dumps(tr)}")
+    dg = DeviceGraph(g)
+    cands = {"committed": MODEL_DIR, "new": os.path.join(outdir, "new", "order_model") + "/"}
+    val_res = {}
+    for name, path in cands.items():
+        m = OrderModel.load(path)
+        sm, _ = compare_orders(dg, g, val, m)
+        m.free()
+        val_res[name] = sm
+        log(f"validation {name}: {json.dumps(sm)}")
+    pick = max(val_res, key=lambda n: val_res[n]["median_speedup_device"] or 0.0)
+    m = OrderModel.load(cands[pick])
+    summary, rows = compare_orders(dg, g, test, m)
+    m.free()
+    summary["model"] = pick
+    summary["validation"] = val_res
+    summary["seconds"] = time.time() - t0
+    log(f"test ({pick}): {json.dumps(summary)}")
+    with open(os.path.join(outdir, "order_eval.json"), "w") as f:
         json.dump({"summary": summary, "rows": rows}, f)
+    dg.free()
     return summary
 
 
@@ -331,8 +452,9 @@ def main(argv):
     if len(argv) >= 2 and argv[0] == "train-order":
         train_order(argv[1], n_train=int(argv[2]) if len(argv) > 2 else 8000)
         return 0
-    if len(argv) >= 3 and argv[0] == "eval-order":
-        eval_order(argv[1], argv[2], n_eval=int(argv[3]) if len(argv) > 3 else 2000)
+    if len(argv) >= 2 and argv[0] == "c4":
+        c4_pipeline(argv[1], n_train=int(argv[2]) if len(argv) > 2 else 6000,
+                    log=lambda m: print(m, flush=True))
         return 0
     if len(argv) >= 3 and argv[0] == "eval-batch":
         eval_batch(argv[1], argv[2])

@@ -292,6 +292,12 @@ def test_batch_orders_level_rows_and_budget(c1):
     for cb, cs_ in zip(counts_b, singles):
         assert cb == cs_ or cb == 2 ** 64 - 1
     assert any(cb == 2 ** 64 - 1 for cb in counts_b)
+    # Lane tables of 64 rows: most queries overflow their lane and are counted
+    # again on the chunked path, where the budget must mark them the same way
+    # instead of failing the whole batch.
+    counts_o, _, st = dg.batch_count_orders(qs, [mg.plan_order(x) for x in qs],
+                                            max_elements=max(budget, 1), chunk_rows=64)
+    assert counts_o.tolist() == counts_b.tolist()
 
 
 @pytest.fixture(scope="module")
