@@ -345,6 +345,9 @@ def batched_workload(g, dg, oracle_counts=None):
         assert counts == ref_counts, name
         out[name] = {"seconds": wall, "queries_per_s": len(qs) / wall}
         _log(f"batched {name}: {wall:.2f} s")
+    t0 = time.perf_counter()
+    dg.plan_orders(qs, order="learned", model=model)
+    out["batch_learned"]["planning_seconds"] = time.perf_counter() - t0
     base = out["per_query_reference"]["seconds"]
     for name in ("batch_reference", "batch_learned"):
         out[name]["speedup_vs_per_query_reference"] = base / out[name]["seconds"]
@@ -604,15 +607,23 @@ def run_mine(args):
     e2e_times = []
     h2d = (g.n + 1) * 4 + g.m_out * 4 + 4 * g.n * 3 + sum(q.n * 4 * 4 + q.m_out * 8 for q in qs)
     d2h = 8 * len(qs)
+    e2e_parts = []
     for _ in range(args.e2e_steps):
         torch.cuda.synchronize(device)
         t0 = time.perf_counter()
         dg2 = mg.DeviceGraph(g, device)
+        t1 = time.perf_counter()
         for q in qs:
             dg2.count(q, **shard)
+        t2 = time.perf_counter()
         dg2.free()
-        e2e_times.append(time.perf_counter() - t0)
+        t3 = time.perf_counter()
+        e2e_times.append(t3 - t0)
+        e2e_parts.append((t1 - t0, t2 - t1, t3 - t2))
     e2e_s = statistics.median(e2e_times) if e2e_times else float("nan")
+    e2e_split = ({"upload_s": statistics.median(p[0] for p in e2e_parts),
+                  "counts_s": statistics.median(p[1] for p in e2e_parts),
+                  "free_s": statistics.median(p[2] for p in e2e_parts)} if e2e_parts else None)
     _log("end-to-end runs done")
     if world > 1:
         t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{device}")
@@ -683,7 +694,8 @@ def run_mine(args):
                 "same_work": same,
                 "e2e": ({"value": emb / e2e_s, "unit": "embeddings/s",
                          "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                         "seconds_per_step": e2e_s} if e2e_times else None),
+                         "seconds_per_step": e2e_s, "split": e2e_split}
+                        if e2e_times else None),
                 "clocks": clocks, "gpu_launches": launches * args.steps,
                 "batched": batch, "learned_order_heldout": heldout, "gar_match": gar,
                 "c5": c5,

@@ -283,39 +283,9 @@ def heldout_split(rec):
     return qs[0::2], qs[1::2]
 
 
-def compare_orders(dg: DeviceGraph, g, recs, model, budget: int = EVAL_BUDGET):
-    """Learned against reference order on the queries of `recs` (selection
-    records with seed and count): both orders planned for the whole set in one
-    call each (the learned one through one inference launch: its time is the
-    planning cost), every query counted under both with the same element
-    budget, and counts checked against the recorded ones.  An order past the
-    budget is censored: a censored reference against a finished learned order
-    is a win, the reverse a loss, and queries censored under both are left out of the medians.  A censored run
-    reports no time, so its time is estimated as the budget at the finished
-    order's measured elements per ms."""
-    import time
-    qs = [learned_query(g, r["seed"]) for r in recs]
-    ref_orders = dg.plan_orders(qs, order="reference")
-    t0 = time.perf_counter()
-    lrn_orders = dg.plan_orders(qs, order="learned", model=model)
-    plan_ms = 1e3 * (time.perf_counter() - t0) / max(1, len(qs))
-    rows = []
-    for r, q, ro, lo in zip(recs, qs, ref_orders, lrn_orders):
-        row = {"seed": r["seed"], "k": q.n, "count": r["count"], "order_ref": ro,
-               "order_learned": lo}
-        for name, od in (("ref", ro), ("learned", lo)):
-            try:
-                c, st = dg.count(q, stats=True, given_order=od, max_elements=budget)
-                assert c == r["count"], (r["seed"], name, c, r["count"])
-                row[f"ms_{name}"] = st["device_ms"]
-                row[f"elements_{name}"] = st["elements"]
-                row[f"done_{name}"] = True
-            except L.MGError as e:
-                if e.code != L.MG_E_LIMIT:
-                    raise
-                row[f"ms_{name}"] = None
-                row[f"done_{name}"] = False
-        rows.append(row)
+def order_summary(rows, budget: int, plan_ms: float) -> dict:
+    """Medians of the learned-over-reference speed-up of compare_orders rows
+    (see there for the censoring rule)."""
     # A censored run reports no time, so a censored order is charged the
     # budget at the finished order's measured elements per ms.
     sp, sp_plan, el = [], [], []
@@ -356,7 +326,43 @@ def compare_orders(dg: DeviceGraph, g, recs, model, budget: int = EVAL_BUDGET):
                "planning_ms_per_query": plan_ms,
                "censoring": "an order past the budget is charged the budget at the other "
                             "order's measured elements per ms (an estimate, not a time)"}
-    return summary, rows
+    return summary
+
+
+def compare_orders(dg: DeviceGraph, g, recs, model, budget: int = EVAL_BUDGET):
+    """Learned against reference order on the queries of `recs` (selection
+    records with seed and count): both orders planned for the whole set in one
+    call each (the learned one through one inference launch: its time is the
+    planning cost), every query counted under both with the same element
+    budget, and counts checked against the recorded ones.  An order past the
+    budget is censored: a censored reference against a finished learned order
+    is a win, the reverse a loss, and queries censored under both are left out of the medians.  A censored run
+    reports no time, so its time is estimated as the budget at the finished
+    order's measured elements per ms."""
+    import time
+    qs = [learned_query(g, r["seed"]) for r in recs]
+    ref_orders = dg.plan_orders(qs, order="reference")
+    t0 = time.perf_counter()
+    lrn_orders = dg.plan_orders(qs, order="learned", model=model)
+    plan_ms = 1e3 * (time.perf_counter() - t0) / max(1, len(qs))
+    rows = []
+    for r, q, ro, lo in zip(recs, qs, ref_orders, lrn_orders):
+        row = {"seed": r["seed"], "k": q.n, "count": r["count"], "order_ref": ro,
+               "order_learned": lo}
+        for name, od in (("ref", ro), ("learned", lo)):
+            try:
+                c, st = dg.count(q, stats=True, given_order=od, max_elements=budget)
+                assert c == r["count"], (r["seed"], name, c, r["count"])
+                row[f"ms_{name}"] = st["device_ms"]
+                row[f"elements_{name}"] = st["elements"]
+                row[f"done_{name}"] = True
+            except L.MGError as e:
+                if e.code != L.MG_E_LIMIT:
+                    raise
+                row[f"ms_{name}"] = None
+                row[f"done_{name}"] = False
+        rows.append(row)
+    return order_summary(rows, budget, plan_ms), rows
 
 
 def c4_pipeline(outdir: str, n_train: int = 6000, select_seconds: float = 300.0, log=print):

@@ -104,37 +104,54 @@ def test_committed_model_loads_and_keeps_counts_exact(setup):
     model.free()
 
 
-def test_committed_model_cuts_work_on_held_out_queries():
-    """The committed network's orders expand fewer candidate elements in total
-    than the reference order on held-out queries (seeds from 200000, k 6-10)
-    of the scale-20 graph; element counts are exact, so the check is
-    deterministic.  Queries past the budget under either order are skipped."""
+def test_committed_evaluation_reproduces_on_held_out_queries():
+    """The first held-out test queries of the committed evaluation
+    (data/heldout_seeds.json, data/order_eval.json) counted again under the
+    reference order and the committed network's order: the same queries
+    finish within the budget, with the recorded counts and candidate-element
+    totals (element counts are exact, so this is deterministic), and the
+    learned orders expand fewer elements than the reference orders over the
+    queries both finish, as recorded."""
+    import json
+
     from matrixgraph_b200 import _lib as L
     from matrixgraph_b200 import workloads as W
-    if not os.path.exists(MODEL_DIR + "embedding.bin"):
-        pytest.skip("no trained model committed")
-    g = W.rmat_graph(20)
+    ev_path = os.path.join(os.path.dirname(mg.__file__), "data", "order_eval.json")
+    if not (os.path.exists(MODEL_DIR + "embedding.bin") and os.path.exists(W.HELDOUT_SEEDS)
+            and os.path.exists(ev_path)):
+        pytest.skip("no committed held-out evaluation")
+    with open(W.HELDOUT_SEEDS) as f:
+        test, _ = W.heldout_split(json.load(f))
+    with open(ev_path) as f:
+        rows = json.load(f)["rows"]
+    n = min(32, len(test))
+    assert n >= 8 and [r["seed"] for r in rows[:n]] == [r["seed"] for r in test[:n]]
+    g = W.rmat_graph(22)
     dg = mg.DeviceGraph(g)
     model = OM.OrderModel.load(MODEL_DIR)
-    qs = [W.learned_query(g, W.EVAL_FIRST_SEED + i) for i in range(96)]
-    ref = dg.plan_orders(qs, order="reference")
+    qs = [W.learned_query(g, r["seed"]) for r in test[:n]]
     lrn = dg.plan_orders(qs, order="learned", model=model)
-    el_ref = el_lrn = both = 0
-    for q, ro, lo in zip(qs, ref, lrn):
-        try:
-            c1, s1 = dg.count(q, stats=True, given_order=ro, max_elements=1 << 27)
-            c2, s2 = dg.count(q, stats=True, given_order=lo, max_elements=1 << 27)
-        except L.MGError as e:
-            assert e.code == L.MG_E_LIMIT
-            continue
-        assert c1 == c2
-        el_ref += s1["elements"]
-        el_lrn += s2["elements"]
-        both += 1
     model.free()
+    el = {"ref": 0, "learned": 0}
+    for q, rec, lo in zip(qs, rows[:n], lrn):
+        assert lo == rec["order_learned"], rec["seed"]
+        assert mg.plan_order(q) == rec["order_ref"], rec["seed"]
+        both = rec["done_ref"] and rec["done_learned"]
+        for name, od in (("ref", rec["order_ref"]), ("learned", lo)):
+            try:
+                c, st = dg.count(q, stats=True, given_order=od, max_elements=W.EVAL_BUDGET)
+                done = True
+            except L.MGError as e:
+                assert e.code == L.MG_E_LIMIT
+                done = False
+            assert done == rec[f"done_{name}"], (rec["seed"], name)
+            if done:
+                assert c == rec["count"], (rec["seed"], name)
+                assert st["elements"] == rec[f"elements_{name}"], (rec["seed"], name)
+                if both:
+                    el[name] += st["elements"]
     dg.free()
-    assert both >= 48, both
-    assert el_lrn < el_ref, (el_lrn, el_ref)
+    assert el["learned"] < el["ref"], el
 
 
 def _numpy_features(g, q):
