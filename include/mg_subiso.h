@@ -387,6 +387,8 @@ int  mg_matrix_filter_keep(void* filter, uint32_t u, const uint32_t* v, uint64_t
  * match count is reachable (more, smaller chunks).  A caller-set chunk_rows
  * whose tables do not fit is rejected with MG_E_LIMIT.  The data graph must
  * already be resident (mg_graph_upload); orders: reference, strong, given.
+ * The closed-form pendant tail is not used (its aggregate tables would need
+ * scratch of their own), so no_tail is ignored; counts are the same.
  * The first call on a device looks up the array's device address with that
  * device current; make that first call before any stream capture.  Every
  * call shares the array and leaves its contents behind (counters are
