@@ -112,7 +112,7 @@ def config(scale, n, m, only=""):
 # the one-pass ncu launch list summarised in
 # profiles/launches_rmat22_5queries_traffic.md (mean over the expand launches
 # of one step).
-EXPAND_TRAFFIC_BYTES = 230_592_092
+EXPAND_TRAFFIC_BYTES = 233_955_702
 
 
 def peaks():
