@@ -317,6 +317,59 @@ def c3_oracle_sample(g, og, every=32, max_elements=10 ** 7, max_count=10 ** 8):
     return {i: O.count(og, O.query_from_csr(qs[i]), threads=threads)["count"] for i in picked}
 
 
+def c1_inputs():
+    """Configuration C1: Chung-Lu (10,000 vertices, exponent 2.5, mean degree
+    10, seed 0, 8 uniform labels, seed 1) and a 4-cycle with labels uniform
+    over the 8 (seed 2)."""
+    import matrixgraph_b200 as mg
+    g = mg.chung_lu()
+    q = mg.CSRGraph.query(4, SHAPES["4-cycle"][1], mg.gen_labels(4, 8, "uniform", seed=2))
+    return g, q
+
+
+def c1_oracle_run(threads):
+    """The oracle's count and sorted rows of C1 (CPU leg, timed)."""
+    import oracle as O
+    g, q = c1_inputs()
+    og, oq = O.Graph.from_csr(g), O.query_from_csr(q)
+    t0 = time.perf_counter()
+    c = O.count(og, oq, threads=threads)["count"]
+    t1 = time.perf_counter()
+    rows = O.emit(og, oq)
+    return {"count": c, "rows": rows, "count_s": t1 - t0, "emit_s": time.perf_counter() - t1,
+            "threads": threads}
+
+
+def c1_workload(device, oracle_res):
+    """C1 on the GPU: upload, count and emit (device time of each from the
+    library's events, median of 5 after a warm-up), compared with the
+    oracle's count and sorted rows."""
+    import numpy as np
+
+    import matrixgraph_b200 as mg
+    g, q = c1_inputs()
+    dg = mg.DeviceGraph(g, device)
+    cnt_ms, emit_ms = [], []
+    for _ in range(6):
+        c, st = dg.count(q, stats=True)
+        cnt_ms.append(st["device_ms"])
+        rows, _, st2 = dg.emit(q, stats=True)
+        emit_ms.append(st2["device_ms"])
+    dg.free()
+    out = {"workload": "Chung-Lu n=10,000 (exponent 2.5, mean degree 10, 8 uniform labels), "
+                       "labelled 4-cycle; count and sorted emit",
+           "count": int(c), "rows": int(len(rows)),
+           "gpu_count_ms": statistics.median(cnt_ms[1:]),
+           "gpu_emit_ms": statistics.median(emit_ms[1:])}
+    if oracle_res is not None:
+        out.update({"oracle_count": oracle_res["count"],
+                    "equal": int(c) == oracle_res["count"] and
+                    np.array_equal(rows, oracle_res["rows"]),
+                    "cpu_count_s": oracle_res["count_s"], "cpu_emit_s": oracle_res["emit_s"],
+                    "cpu_threads": oracle_res["threads"]})
+    return out
+
+
 def batched_workload(g, dg, oracle_counts=None):
     """The 4,096-query batch on the same resident graph: the per-query
     heuristic-order form (one call per query) against batched calls — the
@@ -534,7 +587,7 @@ def run_mine(args):
     gen_s = time.perf_counter() - t0
     _log("workload generated")
     # The oracle runs before this process initialises CUDA.
-    cpu, cpu_rows, c3_oracle = None, None, None
+    cpu, cpu_rows, c3_oracle, c1_oracle = None, None, None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle as O
         threads = os.cpu_count() or 1
@@ -543,6 +596,8 @@ def run_mine(args):
         cpu_rows = oracle_sample(og, oqs, names, threads)
         if not args.no_batch and args.scale == 22 and not args.queries:
             c3_oracle = c3_oracle_sample(g, og)
+        if not args.queries:
+            c1_oracle = c1_oracle_run(threads)
         del og
         c, s = sum(r[4] for r in cpu_rows), sum(r[5] for r in cpu_rows)
         cpu = {"value": c / s if s > 0 else 0.0, "unit": "embeddings/s", "cores": threads,
@@ -644,6 +699,11 @@ def run_mine(args):
         same = same_work(dg, qs, names, cpu_rows, device, g)
         _log(f"same-work check: equal={same['equal']}")
 
+    c1 = None
+    if world == 1 and not args.queries:
+        c1 = c1_workload(device, c1_oracle)
+        _log(f"C1 done: equal={c1.get('equal')}")
+
     peak, peak_kind = peaks()
     # The dominant kernel is the expand kernel (over 90% of device time): its
     # algorithmic bytes per launch are the step's B_alg (count-mode
@@ -698,7 +758,7 @@ def run_mine(args):
                         if e2e_times else None),
                 "clocks": clocks, "gpu_launches": launches * args.steps,
                 "batched": batch, "learned_order_heldout": heldout, "gar_match": gar,
-                "c5": c5,
+                "c5": c5, "c1": c1,
                 "graph": {"n": info["n"], "m_out": info["m_out"],
                           "device_bytes": info["device_bytes"], "max_degree": info["max_degree"],
                           "gen_seconds": gen_s}}
@@ -709,6 +769,8 @@ def run_mine(args):
         torch.distributed.destroy_process_group()
     if same is not None and not same["equal"]:
         sys.exit("same-work counts differ from the oracle")
+    if c1 is not None and c1.get("equal") is False:
+        sys.exit("C1 count or rows differ from the oracle")
 
 
 def main():

@@ -112,9 +112,10 @@ typedef struct mg_opts {
   uint64_t mem_budget_bytes; /* cap on enumeration scratch; 0 = auto        */
   uint64_t root_begin;       /* level-0 candidates [root_begin, root_end) of  */
   uint64_t root_end;         /* the first position's label bucket; 0,0 = all  */
-  uint32_t no_tail;          /* closed-form count of a two-position pendant
-                                tail (count mode): 0 or 2 = whenever the plan
-                                ends in one, 1 = never                       */
+  uint32_t no_tail;          /* closed-form count of a two-position ending
+                                (count mode): a pendant path or two leaves of
+                                one anchor; 0 or 2 = whenever the plan ends
+                                in one, 1 = never                            */
   uint32_t lanes;            /* batch counts: queries run as fixed launch
                                 sequences on this many concurrent streams,
                                 every size read on the device, one host sync
@@ -387,8 +388,9 @@ int  mg_matrix_filter_keep(void* filter, uint32_t u, const uint32_t* v, uint64_t
  * match count is reachable (more, smaller chunks).  A caller-set chunk_rows
  * whose tables do not fit is rejected with MG_E_LIMIT.  The data graph must
  * already be resident (mg_graph_upload); orders: reference, strong, given.
- * The closed-form pendant tail is not used (its aggregate tables would need
- * scratch of their own), so no_tail is ignored; counts are the same.
+ * The closed-form two-position endings are not used (the pendant tail's
+ * aggregate tables would need scratch of their own), so no_tail is ignored;
+ * counts are the same.
  * The first call on a device looks up the array's device address with that
  * device current; make that first call before any stream capture.  Every
  * call shares the array and leaves its contents behind (counters are

@@ -79,6 +79,14 @@ struct PlanDev {
   uint32_t tail_Ia;  // positions i < a labelled like position a
   uint32_t tail_J;   // positions j < a labelled like position b
   uint32_t tail_kid; // index of (da, la, db, lb) in the call's tail-key table
+  // Two final leaves of one anchor (count mode): positions k-2 and k-1 each
+  // have the single backward neighbour star_p (< k-2) in direction star_d and
+  // no self-loop, and no edge between them.  A prefix of length k-2 then has
+  // A = |S_a| minus its matches inside S_a choices for k-2 and, for k-1,
+  // A - 1 when both carry one label (the same slice) or the free entries of
+  // the other label's slice; it is counted while position k-3 expands.
+  uint32_t star2;
+  uint32_t star_p, star_d;
 };
 
 // Signature of a two-hop aggregate: A(y) = sum over the da-slice of y labelled

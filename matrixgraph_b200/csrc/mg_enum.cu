@@ -212,6 +212,7 @@ struct StepArgs {
   // position k-3; the two-hop aggregates of a hub m_p are read at
   // tkeys[kid].base + hub slot, those of other vertices summed in place.
   uint32_t tail_dense;
+  uint32_t star;  // two-leaf star endings are counted in closed form (PlanDev::star2)
   const unsigned long long* tdA;
   const unsigned long long* tdAD;
   unsigned long long* tdL;  // lazily filled aggregates of non-hub vertices
@@ -480,6 +481,47 @@ __device__ __forceinline__ void tail_close(const StepArgs& a, const PlanDev& P, 
   cnt = (unsigned long long)c;
   pre = (unsigned long long)(e - s) - inS;
   dsum = (unsigned long long)d;
+}
+
+// Closed-form count of one prefix of length k-2 whose plan ends in two leaves
+// a = k-2, b = k-1 of one anchor p (PlanDev::star2).  S_a and S_b are the
+// label-l_a and label-l_b slices of m_p in direction d; A_x is |S_x| minus the
+// earlier matches labelled l_x that lie in S_x (injectivity).  Then
+//   count = A_a * (A_a - 1)   when l_a == l_b (S_b == S_a, b differs from a),
+//   count = A_a * A_b         otherwise (a and b cannot collide),
+// the prefixes of length k-1 number A_a, and the algorithmic bytes of the two
+// positions are (8 + 4|S_a|) per prefix of length k-2 plus (8 + 4|S_b|) per
+// prefix of length k-1 (count-mode definition: 8 for the last position).
+// col(j) is the vertex matched at position j < k-2.
+template <class Col>
+__device__ __forceinline__ void star_close(const StepArgs& a, const PlanDev& P, Col col,
+                                           unsigned long long& cnt, unsigned long long& pre,
+                                           unsigned long long& bal,
+                                           unsigned long long& balc) {
+  const GraphDev& g = a.g;
+  const uint32_t ia = P.k - 2, ib = P.k - 1, d = P.star_d;
+  const uint32_t mp = col(P.star_p);
+  uint32_t sa, ea;
+  slice_of(g, d, mp, P.label[ia], sa, ea);
+  unsigned long long A = ea - sa;
+  for (uint32_t m = P.samelab[ia]; m; m &= m - 1)
+    if (in_slice_se(g, d, mp, sa, ea, col(__ffs(m) - 1), a.probe_min)) A -= 1;
+  unsigned long long lb_len;
+  if (P.label[ib] == P.label[ia]) {
+    cnt = A ? A * (A - 1) : 0ull;
+    lb_len = ea - sa;
+  } else {
+    uint32_t sb, eb;
+    slice_of(g, d, mp, P.label[ib], sb, eb);
+    unsigned long long B = eb - sb;
+    for (uint32_t m = P.samelab[ib]; m; m &= m - 1)
+      if (in_slice_se(g, d, mp, sb, eb, col(__ffs(m) - 1), a.probe_min)) B -= 1;
+    cnt = A * B;
+    lb_len = eb - sb;
+  }
+  pre = A;
+  bal = 8ull + 4ull * (ea - sa) + A * (8ull + 4ull * lb_len);
+  balc = 8ull + 4ull * (ea - sa) + A * 8ull;
 }
 
 // Work kernel: per row, the driving slice (shortest backward slice, or the
@@ -769,7 +811,8 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
         fin = (i + 1 == P.k);
         if constexpr ((MODE & X_FUSED) != 0)
           fused = !fin && a.count_mode && (i + 2 == P.k) && P.last_o1;
-        if constexpr ((MODE & X_TAIL) != 0) ftail = a.tail_dense && P.tail2 && i + 3 == P.k;
+        if constexpr ((MODE & X_TAIL) != 0)
+          ftail = ((a.tail_dense && P.tail2) || (a.star && P.star2)) && i + 3 == P.k;
         // Filters prune positions whose survivors are extended further; the
         // position before a last position counted in closed form is not
         // filtered (the closed form already yields 0 for hopeless candidates).
@@ -784,6 +827,17 @@ __global__ void __launch_bounds__(EXPAND_BLOCK) k_expand(StepArgs a) {
           s1 += 1;
           if (fin) {
             if (a.count_mode) cnt += 1;
+          } else if ((MODE & X_TAIL) && ftail && P.star2) {
+            // The prefix ending in x has length k-2 and the plan ends in two
+            // leaves of one anchor: counted here, not stored.
+            unsigned long long tc, tp, tb, tbc;
+            star_close(a, P, [&](uint32_t j) { return j == i ? x : a.in.col[j][r]; }, tc, tp,
+                       tb, tbc);
+            cnt += tc;
+            sk += tc;
+            s2 += tp;
+            bal += tb;
+            balc += tbc;
           } else if ((MODE & X_TAIL) && ftail) {
             // The prefix ending in x has length k-2: its two-position pendant
             // tail is counted here from the dense aggregates, not stored.
@@ -1117,6 +1171,17 @@ int build_plan(const DevGraph* dg, const QueryGraph& Q, const uint32_t* order, P
       }
     }
   }
+  if (!P->tail2 && P->last_o1 && k >= 3 && !P->zero) {
+    // Two final leaves of one anchor: k-2 and k-1 have the same single
+    // backward constraint (position and direction), so they are not adjacent.
+    const uint32_t ia = k - 2, cb = P->cons[kl][0];
+    if (P->ncons[ia] == 1 && P->cons[ia][0] == cb && (cb & 0xFF) < ia &&
+        !((P->selfloop_mask >> ia) & 1u)) {
+      P->star2 = 1;
+      P->star_p = cb & 0xFF;
+      P->star_d = cb >> 8;
+    }
+  }
   if (P->last_o1) {
     const uint32_t cs = P->cons[kl][0];
     const uint32_t ws = order[cs & 0xFF], dir = cs >> 8;
@@ -1194,7 +1259,7 @@ static void launch_expand(const StepArgs& a, const PlanDev* plans, uint32_t npla
   for (uint32_t pi = 0; pi < nplans; ++pi) {
     const PlanDev& p = plans[pi];
     if (count_mode && p.k == i + 2 && p.last_o1) fused = true;
-    if (a.tail_dense && p.tail2 && p.k == i + 3) tail = true;
+    if (((a.tail_dense && p.tail2) || (a.star && p.star2)) && p.k == i + 3) tail = true;
     if (!count_mode && p.k == i + 1) emit = true;
   }
   const bool one = nplans == 1 && a.in.qid == nullptr;
@@ -1371,12 +1436,13 @@ static int run_levels(DevGraph* dg, std::vector<PlanDev> plans, bool count_mode,
       MG_CK(cudaMemcpyAsync(ws->plans, plans.data(), nq * sizeof(PlanDev),
                             cudaMemcpyHostToDevice, st));
   }
+  a.star = count_mode && o.no_tail != 1;
   // writes[l]: some query can append rows to the level-(l+1) table.
   bool writes[MAXK] = {};
   for (uint32_t l = 0; l < kmax; ++l)
     for (auto& p : plans)
       if (p.k > l + 1 && !(count_mode && p.k == l + 2 && p.last_o1) &&
-          !(dense && p.tail2 && p.k == l + 3))
+          !(dense && p.tail2 && p.k == l + 3) && !(a.star && p.star2 && p.k == l + 3))
         writes[l] = true;
 
   auto launch_work_scan = [&](int l) -> int {
@@ -1843,10 +1909,10 @@ static int ensure_lanes(DevGraph* dg, uint32_t nl, uint64_t cap, uint32_t kmax) 
 // Last level a plan expands in count mode: k-1, or k-2 when the last
 // position is closed in place, or k-3 when a pendant tail is closed from
 // dense aggregates.
-static int last_level(const PlanDev& P, bool dense) {
+static int last_level(const PlanDev& P, bool dense, bool star) {
   int l = int(P.k) - 1;
   if (P.k >= 2 && P.last_o1) l = int(P.k) - 2;
-  if (dense && P.tail2) l = int(P.k) - 3;
+  if ((dense && P.tail2) || (star && P.star2)) l = int(P.k) - 3;
   return l;
 }
 
@@ -1898,6 +1964,7 @@ static int subiso_batch_lanes(DevGraph* dg, std::vector<PlanDev>& plans, const m
 
   a.g = dg->g;
   a.count_mode = 1;
+  a.star = o.no_tail != 1;
   a.filters = o.filters & MG_FILTER_ALL;
   a.grab = o.grab;
   a.root_step = 1;
@@ -1926,7 +1993,7 @@ static int subiso_batch_lanes(DevGraph* dg, std::vector<PlanDev>& plans, const m
     a.q_elems = L.qel;
     a.scan_status = L.status;
     a.tile_row = L.tile_row;
-    const int last = P.zero ? -1 : last_level(P, a.tail_dense != 0);
+    const int last = P.zero ? -1 : last_level(P, a.tail_dense != 0, a.star != 0);
     for (int l = 0; l <= last; ++l) {
       a.level = uint32_t(l);
       TabPtrs t{};

@@ -429,7 +429,13 @@ void tail_kind(const QueryGraph& Q, const QFeat& f, uint32_t all, uint32_t a, ui
   const uint32_t bb = f.adj[b] & all & ~(1u << b);
   *last_o1 = __builtin_popcount(bb) == 1 && !self_b;
   *tail2 = false;
-  if (!*last_o1 || bb != (1u << a) || self_a) return;
+  if (!*last_o1 || self_a) return;
+  if (bb != (1u << a)) {
+    // two leaves of one anchor p (a's only neighbour in `all` is b's): the
+    // enumerator counts them in closed form too
+    *tail2 = (f.adj[a] & all & ~(1u << a)) == bb;
+    return;
+  }
   const uint32_t rest = all & ~(1u << a) & ~(1u << b);
   const uint32_t ab = f.adj[a] & rest;
   if (__builtin_popcount(ab) != 1) return;
