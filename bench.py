@@ -86,6 +86,8 @@ def parse():
                    help="skip the batched-workload measurement")
     p.add_argument("--hub-bytes", type=int, default=None,
                    help="hub-bitmap budget of the upload (profiling runs; default: library)")
+    p.add_argument("--only-c5", action="store_true",
+                   help="run only the C5 block and print its record (for profiling)")
     p.add_argument("--c5", type=int, default=8,
                    help="C5 (R-MAT scale 26) queries counted after the headline (0: skip)")
     return p.parse_args()
@@ -579,6 +581,9 @@ def run_mine(args):
     import torch
 
     import matrixgraph_b200 as mg
+    if args.only_c5:
+        print(json.dumps(c5_workload(args.c5)), flush=True)
+        return
     world, rank, local = dist_setup()
     device = local
     t0 = time.perf_counter()
