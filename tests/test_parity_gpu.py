@@ -228,6 +228,53 @@ def test_tail_closed_form(seed):
     dg.free()
 
 
+# (k, undirected edges, an order ending in two leaves of one anchor)
+STAR_QUERIES = [
+    (3, [(0, 1), (0, 2)], [0, 1, 2]),                       # wedge, center first
+    (4, [(0, 1), (0, 2), (0, 3)], [0, 3, 1, 2]),            # 3-star
+    (4, [(0, 1), (1, 2), (1, 3)], [0, 1, 2, 3]),            # leaves of a non-first anchor
+    (5, [(0, 1), (1, 2), (2, 0), (0, 3), (0, 4)], [1, 2, 0, 3, 4]),  # triangle + two leaves
+    (5, [(0, 1), (1, 2), (2, 3), (1, 4)], [2, 3, 1, 0, 4]),  # anchor inside the prefix
+]
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_star_closed_form(seed):
+    """Plans ending in two leaves of one anchor, counted in closed form, equal
+    enumeration (counts, P_i, both algorithmic byte counts): leaves with one
+    label and with two labels, directed graphs with self-loops, single and
+    batch paths."""
+    rng = np.random.default_rng(1300 + seed)
+    directed = seed % 2 == 1
+    n = int(rng.integers(10, 40))
+    nl = int(rng.integers(1, 3))
+    edges, labels = random_graph(rng, n, 0.3, nl, directed=directed, self_loops=directed)
+    g = graph(n, edges, labels, symmetric=not directed)
+    dg = mg.DeviceGraph(g)
+    qs, orders, wants = [], [], []
+    for k, qe, od in STAR_QUERIES:
+        ql = rng.integers(0, max(labels) + 1, k).tolist()
+        if seed % 4 == 0:
+            ql[od[-1]] = ql[od[-2]]  # both leaves on one label
+        if directed:
+            qe = [(b, a) if rng.random() < 0.5 else (a, b) for a, b in qe]
+        q = mg.CSRGraph.query(k, qe, ql, directed=directed)
+        want = oracle_count(g, q, order=od)
+        for tail in (1, 2):
+            c, st = dg.count(q, stats=True, given_order=od, no_tail=tail)
+            assert c == want["count"], (k, qe, ql, tail)
+            assert st["level_rows"] == want["level_rows"], (k, qe, ql, tail)
+            assert st["balg_bytes"] == want["balg"], (k, qe, ql, tail)
+            assert st["balg_count_bytes"] == want["balg_count"], (k, qe, ql, tail)
+        qs.append(q)
+        orders.append(od)
+        wants.append(want)
+    counts, rows, _ = dg.batch_count_orders(qs, orders)
+    for q, c, r, w in zip(qs, counts, rows, wants):
+        assert c == w["count"] and r[:q.n + 1].tolist() == w["level_rows"]
+    dg.free()
+
+
 def test_subiso_exec_cli(tmp_path, c1):
     """The C++ subiso_exec (reference flags) over the C-ABI, exact count and rows."""
     import subprocess
