@@ -8,7 +8,10 @@
 // (core/task/gpu_task/gar_match.cu:193-242) calls for the C-ABI
 // matrixgraph_gar_match — without the yaml-based task around it.
 //
-//   ref_gar_match IN OUT
+//   ref_gar_match IN OUT [REPS]
+// With REPS > 1 the call is repeated REPS times on the same inputs and the
+// median wall time of calls 2..REPS (host arrays in and out, as the
+// reference's C-ABI call) is printed to stderr as "ref_gar_match_ms <t>".
 // IN (little-endian): int32 n_vertices, n_edges, p_nodes, p_edges,
 // row_capacity, match_capacity, has_v_id, has_e_label, has_p_edge_label;
 // then uint32 v_id[n_vertices], int32 v_label[n_vertices], uint32
@@ -20,8 +23,11 @@
 // OUT: int32 status, num_conditions, row_size, match_size; then row_size
 // entries each of uint32 pivot, int32 cond_j, pos, offset, count; then uint32
 // matched_v_ids[match_size].  The reference's own log goes to stdout.
+#include <algorithm>
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "core/task/gpu_task/kernel/kernel_gar_match.cuh"
@@ -35,10 +41,11 @@ static bool read_vec(FILE* f, std::vector<T>& v, int n) {
 }
 
 int main(int argc, char** argv) {
-  if (argc != 3) {
-    std::fprintf(stderr, "usage: ref_gar_match IN OUT\n");
+  if (argc != 3 && argc != 4) {
+    std::fprintf(stderr, "usage: ref_gar_match IN OUT [REPS]\n");
     return 2;
   }
+  const int reps = argc == 4 ? std::max(1, std::atoi(argv[3])) : 1;
   FILE* in = std::fopen(argv[1], "rb");
   if (!in) return 2;
   int32_t h[9];
@@ -63,7 +70,19 @@ int main(int argc, char** argv) {
       cnt(pivot.size());
   K::GARMatchArrays out{&num_conditions, pivot.data(), cond.data(), pos.data(), off.data(),
                         cnt.data(), row_cap, &row_size, ids.data(), match_cap, &match_size};
-  const int status = K::GARMatchKernelWrapper::GARMatch(g, p, &out);
+  int status = 0;
+  std::vector<double> ms;
+  for (int rep = 0; rep < reps; ++rep) {
+    num_conditions = row_size = match_size = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    status = K::GARMatchKernelWrapper::GARMatch(g, p, &out);
+    const auto t1 = std::chrono::steady_clock::now();
+    if (rep > 0) ms.push_back(std::chrono::duration<double, std::milli>(t1 - t0).count());
+  }
+  if (!ms.empty()) {
+    std::sort(ms.begin(), ms.end());
+    std::fprintf(stderr, "ref_gar_match_ms %.6f\n", ms[ms.size() / 2]);
+  }
   FILE* o = std::fopen(argv[2], "wb");
   if (!o) return 2;
   const int32_t head[4] = {status, num_conditions, row_size, match_size};

@@ -35,9 +35,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 EXE = os.path.join(ROOT, "oracle", "_ref", "ref_gar_match")
 
 
-def run_reference(g, p, row_cap, match_cap):
+def run_reference(g, p, row_cap, match_cap, reps=1, timing=None):
     """The reference's GARMatchKernelWrapper::GARMatch on (g, p); returns
-    (status, num_conditions, rows[(pivot, cond_j, pos, offset, count)], ids)."""
+    (status, num_conditions, rows[(pivot, cond_j, pos, offset, count)], ids).
+    With reps > 1 the median wall time of the repeated calls is appended to
+    the list `timing` (ms)."""
     n, m, k, pe = g.n_vertices, len(g.e_src), p.n_nodes, len(p.edge_src)
     assert g.v_id is not None and g.e_label is not None and p.edge_label is not None
     with tempfile.TemporaryDirectory() as d:
@@ -49,8 +51,12 @@ def run_reference(g, p, row_cap, match_cap):
                             (p.node_label, "<i4"), (p.edge_src, "<i4"), (p.edge_dst, "<i4"),
                             (p.edge_label, "<i4")):
                 f.write(np.asarray(arr, dtype=dt).tobytes())
-        r = subprocess.run([EXE, fin, fout], capture_output=True, text=True, timeout=300)
+        r = subprocess.run([EXE, fin, fout] + ([str(reps)] if reps > 1 else []),
+                           capture_output=True, text=True, timeout=300)
         assert r.returncode == 0, r.stderr[-2000:]
+        if timing is not None:
+            timing += [float(x.split()[1]) for x in r.stderr.splitlines()
+                       if x.startswith("ref_gar_match_ms ")]
         raw = open(fout, "rb").read()
     status, nc, rs, ms = struct.unpack_from("<4i", raw, 0)
     rows = [struct.unpack_from("<Iiiii", raw, 16 + 20 * i) for i in range(rs)]
@@ -129,3 +135,35 @@ def test_reference_on_a_medium_graph():
         assert got == as_tuple(restated), seed
         if not restated.filters_pruned:
             assert got == as_tuple(gar_match(*_lib_inputs(g, p), rcap, mcap)), seed
+
+
+@needs_ref
+@pytest.mark.parametrize("n,m", [(3000, 30000), (20000, 200000)])
+def test_reference_timed_beside_the_library(n, m):
+    """The reference's GPU GARMatch rebuilt for sm_100a, timed beside
+    matrixgraph_gar_match on the same inputs (host arrays in and out for both,
+    median of repeated calls after a warm-up); prints one JSON line.  Both
+    calls must succeed; equality of the outputs is checked by the tests above
+    where the reference's frontier cap and filters do not act."""
+    import json
+    import time
+    rng = np.random.default_rng(77)
+    g = random_graph(rng, n, m, v_labels=4, e_labels=2, self_loops=0.0)
+    p = random_pattern(rng, 3, 0, v_labels=4, e_labels=2)
+    rcap, mcap = 10 ** 5, 10 ** 7
+    t_ref = []
+    status, nc, rows, ids = run_reference(g, p, rcap, mcap, reps=3, timing=t_ref)
+    assert status == 0 and len(t_ref) == 1
+    args = _lib_inputs(g, p)
+    res = gar_match(*args, rcap, mcap)
+    t_lib = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        res = gar_match(*args, rcap, mcap)
+        t_lib.append(1e3 * (time.perf_counter() - t0))
+    print(json.dumps({"workload": f"random multigraph, {n:,} vertices, {m:,} directed edges, "
+                                  "4 vertex labels, 2 edge labels; 3-edge pattern",
+                      "reference_gar_match_ms": t_ref[0],
+                      "library_gar_match_ms": sorted(t_lib)[1],
+                      "reference_ids": len(ids), "library_ids": int(res.match_size),
+                      "library_matches": int(res.n_matches)}))
