@@ -263,50 +263,54 @@ void add_rows(std::vector<PosValues>& pv, const uint32_t* rows, uint64_t n_rows,
     if (p.v.size() > 2 * p.sorted + (uint64_t(1) << 20)) p.compact();
 }
 
-// Flattening of kernel_gar_match.cu:640-700: pivots ascending by local
-// index; per position the sorted distinct instance ids; rows stop at the
-// row capacity, ids at the id capacity (the row that meets it keeps the ids
-// that fit).
+// The grouped output of gar_match_arrays.h:14-51: one row per (pivot,
+// position), pivots in ascending local-index order and positions 0..k-1 under
+// each, every row a slice of the id pool holding that position's distinct
+// instance ids under that pivot, ascending.  Output stops at the first
+// capacity reached: no row starts once row_capacity rows exist, and the row
+// that reaches match_capacity keeps only the ids that still fit (possibly
+// none) and ends it.
 void flatten(std::vector<PosValues>& pv, const uint32_t* v_id, uint32_t n, const GarOut& out) {
   const uint32_t k = uint32_t(pv.size());
   for (auto& p : pv) p.compact();
   auto inst = [&](uint32_t v) -> uint32_t { return v_id && v < n ? v_id[v] : v; };
+  int rows = 0, ids = 0;
+  // Appends one row; false once the output is complete.
+  auto append = [&](uint32_t pivot, uint32_t pos, const std::vector<uint32_t>& vals) -> bool {
+    if (rows >= out.row_capacity) return false;
+    const int64_t room = std::max<int64_t>(0, int64_t(out.match_capacity) - ids);
+    const int take = int(std::min<int64_t>(room, int64_t(vals.size())));
+    if (out.row_pivot_id) out.row_pivot_id[rows] = pivot;
+    if (out.row_cond_j) out.row_cond_j[rows] = int32_t(pos);
+    if (out.row_pos) out.row_pos[rows] = int32_t(pos);
+    if (out.row_offset) out.row_offset[rows] = ids;
+    if (out.row_count) out.row_count[rows] = take;
+    if (out.matched && take > 0) std::memcpy(out.matched + ids, vals.data(), size_t(take) * 4);
+    ids += take;
+    rows += 1;
+    return rows < out.row_capacity && ids < out.match_capacity;
+  };
+  // Position cursors walk the packed (pivot << 32 | value) lists in step.
   std::vector<size_t> at(k, 0);
   std::vector<uint32_t> vals;
-  int row_size = 0, match_size = 0;
   const auto& piv = pv[0].v;  // (pivot, pivot): one entry per pivot
-  for (size_t pi = 0; pi < piv.size(); ++pi) {
+  bool more = true;
+  for (size_t pi = 0; pi < piv.size() && more; ++pi) {
     const uint64_t pivot = piv[pi] >> 32;
-    for (uint32_t pos = 0; pos < k; ++pos) {
+    for (uint32_t pos = 0; pos < k && more; ++pos) {
       const auto& p = pv[pos].v;
-      size_t a = at[pos];
-      while (a < p.size() && (p[a] >> 32) < pivot) ++a;
-      size_t b = a;
+      size_t c = at[pos];
+      while (c < p.size() && (p[c] >> 32) < pivot) ++c;
       vals.clear();
-      while (b < p.size() && (p[b] >> 32) == pivot) vals.push_back(inst(uint32_t(p[b++])));
-      at[pos] = b;
+      for (; c < p.size() && (p[c] >> 32) == pivot; ++c) vals.push_back(inst(uint32_t(p[c])));
+      at[pos] = c;
       std::sort(vals.begin(), vals.end());
       vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
-      if (row_size >= out.row_capacity) break;
-      const int offset = match_size;
-      int64_t write_n = int64_t(vals.size());
-      if (int64_t(offset) + write_n > int64_t(out.match_capacity))
-        write_n = std::max<int64_t>(0, int64_t(out.match_capacity) - offset);
-      if (out.row_pivot_id) out.row_pivot_id[row_size] = inst(uint32_t(pivot));
-      if (out.row_cond_j) out.row_cond_j[row_size] = int32_t(pos);
-      if (out.row_pos) out.row_pos[row_size] = int32_t(pos);
-      if (out.row_offset) out.row_offset[row_size] = offset;
-      if (out.row_count) out.row_count[row_size] = int32_t(write_n);
-      if (out.matched && write_n > 0)
-        std::memcpy(out.matched + offset, vals.data(), size_t(write_n) * 4);
-      match_size += int(write_n);
-      row_size += 1;
-      if (row_size >= out.row_capacity || match_size >= out.match_capacity) break;
+      more = append(inst(uint32_t(pivot)), pos, vals);
     }
-    if (row_size >= out.row_capacity || match_size >= out.match_capacity) break;
   }
-  if (out.row_size) *out.row_size = row_size;
-  if (out.match_size) *out.match_size = match_size;
+  if (out.row_size) *out.row_size = rows;
+  if (out.match_size) *out.match_size = ids;
   if (out.num_conditions) *out.num_conditions = int(k);
 }
 
