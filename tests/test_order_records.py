@@ -55,3 +55,28 @@ def test_summary_is_what_the_rows_give():
     assert s["n"] == len(ev["rows"])
     assert s["finished_both"] + s["finished_learned_only"] + s["finished_reference_only"] + \
         s["finished_neither"] == s["n"]
+
+
+def test_censoring_rule_of_the_summary():
+    """Queries both orders finish give measured ratios; a censored reference
+    against a finished learned order is charged the budget at the learned
+    order's elements per ms (a win), the reverse a loss, and queries both
+    orders leave unfinished stay out of the medians."""
+    rows = [
+        {"done_ref": True, "done_learned": True, "ms_ref": 4.0, "ms_learned": 2.0,
+         "elements_ref": 400, "elements_learned": 200},
+        {"done_ref": False, "done_learned": True, "ms_ref": None, "ms_learned": 1.0,
+         "elements_learned": 100},
+        {"done_ref": True, "done_learned": False, "ms_ref": 1.0, "ms_learned": None,
+         "elements_ref": 50},
+        {"done_ref": False, "done_learned": False, "ms_ref": None, "ms_learned": None},
+    ]
+    s = W.order_summary(rows, budget=1000, plan_ms=0.0)
+    assert (s["finished_both"], s["finished_learned_only"], s["finished_reference_only"],
+            s["finished_neither"]) == (1, 1, 1, 1)
+    # ratios: 2.0 (both), 1000/(100 per ms)/1 ms = 10.0 (win), 1 ms/(1000/50 ms) = 0.05 (loss)
+    assert abs(s["median_speedup_device"] - 2.0) < 1e-12
+    assert abs(s["median_speedup_device_both_finished"] - 2.0) < 1e-12
+    assert abs(s["median_element_ratio_both_finished"] - 2.0) < 1e-12
+    s2 = W.order_summary(rows, budget=1000, plan_ms=1.0)
+    assert abs(s2["median_speedup_with_planning"] - 4.0 / 3.0) < 1e-12
