@@ -704,9 +704,23 @@ def run_mine(args):
         same = same_work(dg, qs, names, cpu_rows, device, g)
         _log(f"same-work check: equal={same['equal']}")
 
+    # Blocks after the headline: an exception is recorded in the line instead
+    # of losing it; a failed parity check (AssertionError) also makes the
+    # process exit non-zero once the line is printed.
+    failures = []
+
+    def guarded(name, fn):
+        try:
+            return fn()
+        except Exception as e:
+            _log(f"{name} failed: {e!r}")
+            if isinstance(e, AssertionError):
+                failures.append(f"{name}: {e!r}")
+            return {"error": repr(e)}
+
     c1 = None
     if world == 1 and not args.queries:
-        c1 = c1_workload(device, c1_oracle)
+        c1 = guarded("C1", lambda: c1_workload(device, c1_oracle))
         _log(f"C1 done: equal={c1.get('equal')}")
 
     peak, peak_kind = peaks()
@@ -729,24 +743,21 @@ def run_mine(args):
                 "step_rate_gbs": balgc / (ms_step / 1e3) / 1e9}
     batch = None
     if world == 1 and not args.no_batch and args.scale == 22 and not args.queries:
-        batch = batched_workload(g, dg, c3_oracle)
+        batch = guarded("batched", lambda: batched_workload(g, dg, c3_oracle))
         _log("batched workload done")
     heldout = None
     if world == 1 and not args.no_batch and args.scale == 22 and not args.queries:
-        heldout = heldout_eval(dg, g)
+        heldout = guarded("held-out", lambda: heldout_eval(dg, g))
         _log("held-out order evaluation done")
     c5 = None
     if world == 1 and args.c5 > 0 and not args.queries:
         dg.free()
-        c5 = c5_workload(args.c5)
+        c5 = guarded("C5", lambda: c5_workload(args.c5))
         _log("C5 workload done")
     gar = None
     if world == 1 and not args.no_gar:
-        try:
-            gar = gar_workload()
-            _log("gar workload done")
-        except Exception as e:  # reported in the line, the headline stands
-            gar = {"error": repr(e)}
+        gar = guarded("GAR", gar_workload)
+        _log("gar workload done")
     if rank == 0:
         line = {"metric": "exact embeddings/s", "value": value, "unit": "embeddings/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -776,6 +787,11 @@ def run_mine(args):
         sys.exit("same-work counts differ from the oracle")
     if c1 is not None and c1.get("equal") is False:
         sys.exit("C1 count or rows differ from the oracle")
+    c5_parity = (c5 or {}).get("parity") or {}
+    if c5_parity.get("samples") and not c5_parity.get("all_equal"):
+        sys.exit("C5 fixture counts or rows differ from the oracle")
+    if failures:
+        sys.exit("; ".join(failures))
 
 
 def main():
